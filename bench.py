@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 explicit residual-and-update path.
+
+Workload (the configuration the headline metric is quoted on): 3D Euler
+isentropic vortex (strength 5, gamma 1.4, freestream rho = p = 1,
+u = v = w = 1) on the periodic box [-5,5]^3 split into 8 uneven blocks
+(2,097,152 cells, 3 ghost layers, non-conforming block interfaces), WENO5 +
+AUSM, classic RK4, CFL 0.5. Inputs are the seeded analytic initial state
+(no dataset exists for this solver).
+
+One "step" is one RK4 time step (4 stages) over all blocks. value = cells x
+stages x ranks / max-over-ranks device time, in Gcell-stage/s. The headline
+form computes reconstruction and flux in FP32 with FP64 state and RK
+accumulation; the FP64 plain forms are reported beside it, with the L1
+density difference of the FP32 form against FP64 after the same steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "fvm-3d-f90_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "Gcell-stage/s FP64 plain vs FP32-batched at L1 err<=1e-6; served p50/p99 latency"
+UNIT = "Gcell-stage/s"
+WORKLOAD = "isentropic vortex 3D Euler, periodic [-5,5]^3, 8 uneven blocks, 128^3 = 2,097,152 cells, WENO5 + AUSM, RK4, CFL 0.5"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="product", choices=["product", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="global grid edge (cells)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            # one process per GPU; the library uses the first visible device
+            if "CUDA_VISIBLE_DEVICES" not in os.environ:
+                os.environ["CUDA_VISIBLE_DEVICES"] = str(self.local)
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks + throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: str | None):
+        self.rows = []
+        self.proc = None
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if index is not None:
+            cmd += ["-i", index]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "", 1).isdigit()]
+        pw = [float(r[3]) for r in self.rows if r[3].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "samples": len(self.rows), "reasons": reasons}
+
+
+def bus_id() -> str | None:
+    try:
+        rt = ctypes.CDLL("libcudart.so.12")
+        buf = ctypes.create_string_buffer(64)
+        if rt.cudaDeviceGetPCIBusId(buf, 64, 0) == 0:
+            return buf.value.decode()
+    except OSError:
+        pass
+    return None
+
+
+def peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "src": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+# ---------------------------------------------------------------- product arm
+def product(args, dist: Dist):
+    import numpy as np
+
+    from fvm3d import abi, cases, tuning
+    from fvm3d.solver import Solver
+
+    case = cases.isentropic_vortex(N=args.n, layout="blocks8")
+    ncells = case.ncells
+    stages = 4
+    nblk = len(case.blocks)
+
+    def fresh(prec, tile=None, z=None):
+        s = Solver(case.config(precision=prec))
+        case.apply(s, states=False)
+        if tile is not None:
+            tuning.set_tuning(s, 0, tile, z)
+        for b, q in enumerate(case.states):
+            s.set_state(b, q)
+        return s
+
+    def tune(prec):
+        s = fresh(prec)
+        t, z, ms = tuning.autotune(s, ncells, use_cache=False, reps=2)
+        s.close()
+        return t, z
+
+    def timed(prec):
+        tile, z = tune(prec)
+        s = fresh(prec, tile, z)
+        s.step(args.warmup)
+        dist.barrier()
+        clk = Clocks(bus_id()) if dist.rank == 0 else None
+        ms = tuning.time_step(s, args.steps)
+        clocks = clk.stop() if clk else None
+        ms_max = dist.max(ms)
+        prof = []
+        for _ in range(3):
+            prof.append(tuning.profile_step(s))
+        launches = tuning.launches_per_step(s)
+        return s, ms_max, clocks, prof, launches, (tile, z)
+
+    out = {}
+    s32, ms32, clocks, prof32, launches, tz32 = timed(abi.PREC_FP32_FLUX)
+    s64, ms64, _, prof64, _, tz64 = timed(abi.PREC_FP64)
+    sx, msx, _, profx, _, tzx = timed(abi.PREC_FP64_EXACT)
+
+    def gcs(ms):
+        return ncells * stages * dist.world / (ms * 1e-3) / 1e9
+
+    # L1 density difference of the FP32-flux form against FP64 after the same steps
+    l1 = float(np.mean([np.abs(s32.get_state(b)[0] - s64.get_state(b)[0]).mean() for b in range(nblk)]))
+    l1x = float(np.mean([np.abs(s64.get_state(b)[0] - sx.get_state(b)[0]).mean() for b in range(nblk)]))
+
+    # roofline of the dominant kernel (the fused stage): algorithmic bytes are
+    # the FP64 state arrays each stage must read or write: RK4 stages touch
+    # 3, 5, 5, 4 arrays of 5 x 8 B per cell = 680 B per cell-step.
+    def roof(prof):
+        st = [ms for p in prof for k, ms in p if k == "stage"]
+        per_step_ms = sum(st) / len(prof)
+        alg = 680.0 * ncells
+        ach = alg / (per_step_ms * 1e-3) / 1e9
+        pk = peaks()
+        share = per_step_ms / (sum(ms for p in prof for _, ms in p) / len(prof))
+        return {"bound": "hbm", "achieved": round(ach, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": round(ach / pk["hbm_gbs"], 4), "traffic": None, "peak_src": pk["src"],
+                "stage_ms_per_step": round(per_step_ms, 4), "stage_share_of_step": round(share, 4),
+                "alg_bytes_per_cell_step": 680}
+
+    out["value"] = gcs(ms32)
+    out["ms_per_step"] = ms32
+    out["roofline"] = roof(prof32)
+    out["clocks"] = clocks
+    out["gpu_launches"] = launches * args.steps
+    out["fp64_plain"] = {"value": gcs(ms64), "ms_per_step": ms64, "roofline": roof(prof64), "tile_zchunk": tz64,
+                         "l1_density_vs_fp64_exact": l1x}
+    out["fp64_exact"] = {"value": gcs(msx), "ms_per_step": msx, "roofline": roof(profx), "tile_zchunk": tzx}
+    out["l1_density_err_vs_fp64"] = l1
+    out["tile_zchunk"] = tz32
+    out["profile_ms"] = {k: round(sum(ms for p in prof32 for kk, ms in p if kk == k) / len(prof32), 4)
+                         for k in ("stage", "gather", "finalize")}
+    sx.close()
+    s64.close()
+
+    # end to end through the C ABI with host buffers: every step uploads the
+    # state from pinned host memory, advances one step (residuals come back)
+    # and downloads the state.
+    if not args.no_e2e:
+        import torch
+
+        pins = []
+        for q in case.states:
+            t = torch.empty(q.size, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = q.reshape(-1)
+            pins.append(t)
+        s = fresh(abi.PREC_FP32_FLUX, *tz32)
+        for b, t in enumerate(pins):  # warm-up
+            s.set_state_ptr(b, t.data_ptr())
+        s.step(1)
+        ke = max(3, min(args.steps, 10))
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            for b, t in enumerate(pins):
+                s.set_state_ptr(b, t.data_ptr())
+            s.step(1)
+            for b, t in enumerate(pins):
+                s.get_state_ptr(b, t.data_ptr())
+        sec = (time.perf_counter() - t0) / ke
+        sec = dist.max(sec)
+        out["e2e"] = {"value": ncells * stages * dist.world / sec / 1e9, "unit": UNIT,
+                      "h2d_bytes_per_step": ncells * 40, "d2h_bytes_per_step": ncells * 40 + 2 * 6 * 8 + 8,
+                      "ms_per_step": sec * 1e3,
+                      "path": "fvm_set_state x8 (pinned) + fvm_step(1) + fvm_get_state x8 per step"}
+        s.close()
+    s32.close()
+    return out
+
+
+# ---------------------------------------------------------------- CPU oracle
+def cpu_oracle(n, steps, warmup, threads=None):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from fvm3d import cases
+
+    threads = threads or os.cpu_count() or 1
+    orc.set_threads(threads)
+    case = cases.isentropic_vortex(N=n, layout="blocks8")
+    o = case.apply(orc.Oracle(case.config()))
+    if warmup:
+        o.step(warmup)
+    t0 = time.perf_counter()
+    o.step(steps)
+    sec = time.perf_counter() - t0
+    return case.ncells * 4 * steps / sec / 1e9, threads, sec
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    base = {"metric": METRIC, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells_per_gpu": args.n ** 3, "blocks": 8, "stages_per_step": 4,
+                       "parallelism": f"replicas{dist.world}",
+                       "l2": "inputs larger than L2 (state buffers 4 x 84 MB per GPU)"}}
+    if args.impl == "reference":
+        if dist.rank != 0:
+            dist.close()
+            return
+        v, th, sec = cpu_oracle(args.n, args.steps, args.warmup)
+        line = dict(base)
+        line.update({"impl": "reference", "value": v, "ms_per_step": sec / args.steps * 1e3, "dtype": "f64",
+                     "n_gpus": dist.world,
+                     "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                                      "sample": f"{args.steps} RK4 steps of the full 8-block {args.n}^3 case "
+                                                "(C++ restatement of the reference path, OpenMP)"},
+                     "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        print(json.dumps(line))
+        dist.close()
+        return
+
+    res = product(args, dist)
+    line = dict(base)
+    line.update({"value": res.pop("value"), "ms_per_step": res.pop("ms_per_step"),
+                 "dtype": "f32 recon/flux, f64 state + RK + dt + norms"})
+    line.update(res)
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
+        v, th, sec = cpu_oracle(args.n, 2, 0)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
+                                "sample": "2 RK4 steps of the full 8-block case on all host threads "
+                                          f"({sec:.1f} s; C++ restatement of the reference path)"}
+    if dist.rank == 0:
+        print(json.dumps(line))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

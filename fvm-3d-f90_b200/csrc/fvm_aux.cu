@@ -1,0 +1,320 @@
+// fvm_aux.cu — the kernels around the fused stage: ghost gather, state
+// pack/unpack, primitive download, CFL wave-speed reduction, the per-step
+// finalize (residual norms, time, next dt) and the viscous contribution.
+// Compiled with -fmad=false: every FP64 expression here keeps the
+// reference's rounding order.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fvm_aux.h"
+#include "fvm_schemes.cuh"
+#include "fvm_types.h"
+
+namespace fvm {
+
+// ---------------------------------------------------------------- gather
+// Ghost cells of connected / periodic regions: dst[i] = src[i] for all five
+// variables, offsets relative to a role slab (the block-to-block exchange the
+// reference describes in defs_face_geom.f90:378-402 but never performs).
+__global__ void gather_kernel(double* __restrict__ base, int64_t vs, const int64_t* __restrict__ pairs,
+                              int64_t npairs) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npairs;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = pairs[2 * i], s = pairs[2 * i + 1];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) base[d + v * vs] = base[s + v * vs];
+  }
+}
+
+// ---------------------------------------------------------------- pack / unpack
+// Host layout: Fortran (ni,nj,nk,5) of the real range, get_q()
+// (defs_block_data.f90:299-312).
+__global__ void unpack_kernel(double* __restrict__ role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk,
+                              const double* __restrict__ host_layout) {
+  const int64_t nc = (int64_t)ni * nj * nk;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % ni);
+    const int64_t r = c / ni;
+    const int j = (int)(r % nj), k = (int)(r / nj);
+    const int64_t o = i + (int64_t)j * sy + (int64_t)k * sz;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) role_blk[o + v * vs] = host_layout[c + v * nc];
+  }
+}
+
+__global__ void pack_kernel(const double* __restrict__ role_blk, int64_t vs, int sy, int sz, int ni, int nj,
+                            int nk, double* __restrict__ host_layout, int prim, double gm1) {
+  const int64_t nc = (int64_t)ni * nj * nk;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % ni);
+    const int64_t r = c / ni;
+    const int j = (int)(r % nj), k = (int)(r / nj);
+    const int64_t o = i + (int64_t)j * sy + (int64_t)k * sz;
+    double q[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) q[v] = role_blk[o + v * vs];
+    if (prim) {
+      // convert_q_to_p_blk_sub (class_flow_field.f90:383-396)
+      Prim5<double> p = cons2prim<double, true>(q[0], q[1], q[2], q[3], q[4], gm1);
+      q[0] = p.r; q[1] = p.u; q[2] = p.v; q[3] = p.w; q[4] = p.p;
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) host_layout[c + v * nc] = q[v];
+  }
+}
+
+// ---------------------------------------------------------------- CFL
+__device__ __forceinline__ double cell_wavespeed(const double q[5], double gamma, double gm1, const double dr[3],
+                                                 int idim) {
+  Prim5<double> p = cons2prim<double, true>(q[0], q[1], q[2], q[3], q[4], gm1);
+  const double c = sqrt(gamma * p.p / p.r);
+  double s = (fabs(p.u) + c) / dr[0] + (fabs(p.v) + c) / dr[1];
+  if (idim == 3) s = s + (fabs(p.w) + c) / dr[2];
+  return s;
+}
+
+// Max wave-speed sum per case over role `role` (max is order-free, so the
+// atomic on the non-negative bit pattern is deterministic).
+__global__ void wavespeed_kernel(const DevBlock* blocks, const DevCase* cases, int role,
+                                 unsigned long long* case_max) {
+  const DevBlock B = blocks[blockIdx.y];
+  const DevCase& C = cases[B.case_id];
+  const int64_t nc = (int64_t)B.n[0] * B.n[1] * B.n[2];
+  double m = 0.0;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % B.n[0]);
+    const int64_t r = c / B.n[0];
+    const int j = (int)(r % B.n[1]), k = (int)(r / B.n[1]);
+    const int64_t o = i + (int64_t)j * B.sy + (int64_t)k * B.sz;
+    double q[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) q[v] = B.q[role][o + v * B.vs];
+    m = fmax(m, cell_wavespeed(q, C.gamma, C.gm1, B.dr, C.idim));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(&case_max[B.case_id], (unsigned long long)__double_as_longlong(m));
+}
+
+// dt of the first step: fix_timestep, or cfl / max wave-speed sum.
+__global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const unsigned long long* case_max,
+                               int ncases) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncases) return;
+  const DevCase& C = cases[c];
+  st[c].dt = (C.timestep_set == 0) ? C.dt_fixed : C.cfl / __longlong_as_double((long long)case_max[c]);
+}
+
+// ---------------------------------------------------------------- finalize
+// One CTA per case, after the last stage of a step:
+// ClassIteration%reset_residual / compute_residual per block in block order /
+// update (class_iteration.f90, file-local 195-259), time += dt, the stop
+// checks of converged (:180-188) and the next step's dt.
+__global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, DevCaseState* st,
+                                const double* partials, int* counters, int ncounters) {
+  __shared__ double red[6][256];
+  const int c = blockIdx.x, tid = threadIdx.x;
+  const DevCase& C = cases[c];
+  double res[6] = {0, 0, 0, 0, 0, 0};
+  double wmax = 0.0;
+  for (int b = C.block0; b < C.block0 + C.nblocks; ++b) {
+    const DevBlock& B = blocks[b];
+    double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
+    for (int t = tid; t < B.ntask; t += blockDim.x) {
+      const double* p = partials + (int64_t)(B.task0 + t) * kPartStride;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) s[v] += p[v];
+      m = fmax(m, p[5]);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) red[v][tid] = s[v];
+    red[5][tid] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (tid < w) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) red[v][tid] += red[v][tid + w];
+        red[5][tid] = fmax(red[5][tid], red[5][tid + w]);
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
+      double res2[5], res2_t = 0.0;
+      for (int v = 0; v < 5; ++v) {
+        res2[v] = red[v][0] / npt;
+        res2_t = res2_t + res2[v];
+      }
+      res2_t = res2_t / 5.0;
+      for (int v = 0; v < 5; ++v) res[v] = sqrt(res[v] * res[v] + res2[v]);
+      res[5] = sqrt(res[5] * res[5] + res2_t);
+      wmax = fmax(wmax, red[5][0]);
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    DevCaseState& S = st[c];
+    S.step += 1;
+    S.t = S.t + S.dt;
+    S.dt_last = S.dt;
+    for (int e = 0; e < 6; ++e) S.res_abs[e] = res[e];
+    if (S.step == 1)
+      for (int e = 0; e < 6; ++e) S.res_abs0[e] = res[e];
+    for (int e = 0; e < 6; ++e) S.res_rel[e] = S.res_abs[e] / S.res_abs0[e];
+    if (isnan(res[5]))
+      S.status = 4;  // FVM_ERR_NONFINITE
+    else if (res[5] > 1.0E10)
+      S.status = 5;  // FVM_ERR_DIVERGED
+    S.dt = (C.timestep_set == 0) ? C.dt_fixed : C.cfl / wmax;
+  }
+  if (c == 0)
+    for (int i = tid; i < ncounters; i += blockDim.x) counters[i] = 0;
+}
+
+// ---------------------------------------------------------------- viscous
+// Central second-order viscous contribution (the reference's
+// viscous_flux_sub, class_space_discret.f90:671-675, is empty; this is the
+// textbook form): V = (dGx + dGy) + dGz with dG = (G(i+1/2) - G(i-1/2)) / dr.
+struct VPrim {
+  double u, v, w, th;
+};
+
+__device__ __forceinline__ int64_t vcell(const DevBlock& B, int x, int y, int z) {
+  const int m = B.ghost_mask;
+  if (x < 0 && !(m & 1)) x = 0;
+  if (x >= B.n[0] && !(m & 2)) x = B.n[0] - 1;
+  if (y < 0 && !(m & 4)) y = 0;
+  if (y >= B.n[1] && !(m & 8)) y = B.n[1] - 1;
+  if (z < 0 && !(m & 16)) z = 0;
+  if (z >= B.n[2] && !(m & 32)) z = B.n[2] - 1;
+  return x + (int64_t)y * B.sy + (int64_t)z * B.sz;
+}
+
+__device__ __forceinline__ VPrim vprim(const double* q, int64_t o, int64_t vs, double gm1) {
+  Prim5<double> p = cons2prim<double, true>(q[o], q[o + vs], q[o + 2 * vs], q[o + 3 * vs], q[o + 4 * vs], gm1);
+  VPrim r;
+  r.u = p.u;
+  r.v = p.v;
+  r.w = p.w;
+  r.th = p.p / p.r;
+  return r;
+}
+
+__device__ __forceinline__ double vcomp(const VPrim& p, int m) {
+  return m == 0 ? p.u : (m == 1 ? p.v : (m == 2 ? p.w : p.th));
+}
+
+// Viscous flux through the face between cells cL and cL + e_dir.
+__device__ void visc_face(const DevBlock& B, const DevCase& C, const double* q, int dir, int x, int y, int z,
+                          double G[5]) {
+  int e[3] = {0, 0, 0};
+  e[dir] = 1;
+  const double gm1 = C.gm1;
+  const VPrim L = vprim(q, vcell(B, x, y, z), B.vs, gm1);
+  const VPrim R = vprim(q, vcell(B, x + e[0], y + e[1], z + e[2]), B.vs, gm1);
+  double grad[4][3];
+  for (int m = 0; m < 4; ++m)
+    for (int d = 0; d < 3; ++d) grad[m][d] = 0.0;
+  for (int m = 0; m < 4; ++m) grad[m][dir] = (vcomp(R, m) - vcomp(L, m)) / B.dr[dir];
+  for (int d = 0; d < C.idim; ++d) {
+    if (d == dir) continue;
+    int t[3] = {0, 0, 0};
+    t[d] = 1;
+    const VPrim lp = vprim(q, vcell(B, x + t[0], y + t[1], z + t[2]), B.vs, gm1);
+    const VPrim lm = vprim(q, vcell(B, x - t[0], y - t[1], z - t[2]), B.vs, gm1);
+    const VPrim rp = vprim(q, vcell(B, x + e[0] + t[0], y + e[1] + t[1], z + e[2] + t[2]), B.vs, gm1);
+    const VPrim rm = vprim(q, vcell(B, x + e[0] - t[0], y + e[1] - t[1], z + e[2] - t[2]), B.vs, gm1);
+    for (int m = 0; m < 4; ++m)
+      grad[m][d] = ((vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m))) / (4.0 * B.dr[d]);
+  }
+  const double div = grad[0][0] + grad[1][1] + grad[2][2];
+  const double uf[3] = {0.5 * (L.u + R.u), 0.5 * (L.v + R.v), 0.5 * (L.w + R.w)};
+  double tau[3];
+  for (int m = 0; m < 3; ++m) {
+    tau[m] = C.mu * (grad[m][dir] + grad[dir][m]);
+    if (m == dir) tau[m] = tau[m] - 2.0 / 3.0 * C.mu * div;
+  }
+  G[0] = 0.0;
+  G[1] = tau[0];
+  G[2] = tau[1];
+  G[3] = tau[2];
+  G[4] = uf[0] * tau[0] + uf[1] * tau[1] + uf[2] * tau[2] + C.kq * grad[3][dir];
+}
+
+__global__ void visc_kernel(const DevBlock* blocks, const DevCase* cases, int role) {
+  const DevBlock B = blocks[blockIdx.y];
+  const DevCase C = cases[B.case_id];
+  if (!B.visc) return;
+  const double* q = B.q[role];
+  const int64_t nc = (int64_t)B.n[0] * B.n[1] * B.n[2];
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % B.n[0]);
+    const int64_t r = c / B.n[0];
+    const int j = (int)(r % B.n[1]), k = (int)(r / B.n[1]);
+    double V[5] = {0, 0, 0, 0, 0};
+    for (int dir = 0; dir < C.idim; ++dir) {
+      int e[3] = {0, 0, 0};
+      e[dir] = 1;
+      double Gl[5], Gr[5];
+      visc_face(B, C, q, dir, i - e[0], j - e[1], k - e[2], Gl);
+      visc_face(B, C, q, dir, i, j, k, Gr);
+      for (int v = 0; v < 5; ++v) V[v] = V[v] + (Gr[v] - Gl[v]) / B.dr[dir];
+    }
+    const int64_t o = i + (int64_t)j * B.sy + (int64_t)k * B.sz;
+    for (int v = 0; v < 5; ++v) B.visc[o + v * B.vs] = V[v];
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+static inline int grid_for(int64_t n, int bs) {
+  int64_t g = (n + bs - 1) / bs;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+cudaError_t launch_gather(double* base, int64_t vs, const int64_t* pairs, int64_t npairs, cudaStream_t s) {
+  if (npairs == 0) return cudaSuccess;
+  gather_kernel<<<grid_for(npairs, 256), 256, 0, s>>>(base, vs, pairs, npairs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, const double* src,
+                          cudaStream_t s) {
+  unpack_kernel<<<grid_for((int64_t)ni * nj * nk, 256), 256, 0, s>>>(role_blk, vs, sy, sz, ni, nj, nk, src);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, double* dst,
+                        int prim, double gm1, cudaStream_t s) {
+  pack_kernel<<<grid_for((int64_t)ni * nj * nk, 256), 256, 0, s>>>(role_blk, vs, sy, sz, ni, nj, nk, dst, prim,
+                                                                    gm1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* cases, DevCaseState* st, int ncases,
+                           unsigned long long* case_max, int role, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(case_max, 0, sizeof(unsigned long long) * ncases, s);
+  if (e != cudaSuccess) return e;
+  if (nblocks > 0) {
+    dim3 g(64, nblocks);
+    wavespeed_kernel<<<g, 256, 0, s>>>(blocks, cases, role, case_max);
+  }
+  init_dt_kernel<<<(ncases + 127) / 128, 128, 0, s>>>(cases, st, case_max, ncases);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, DevCaseState* st, int ncases,
+                            const double* partials, int* counters, int ncounters, cudaStream_t s) {
+  finalize_kernel<<<ncases, 256, 0, s>>>(blocks, cases, st, partials, counters, ncounters);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_visc(const DevBlock* blocks, int nblocks, const DevCase* cases, int role, cudaStream_t s) {
+  if (nblocks == 0) return cudaSuccess;
+  dim3 g(128, nblocks);
+  visc_kernel<<<g, 128, 0, s>>>(blocks, cases, role);
+  return cudaGetLastError();
+}
+
+}  // namespace fvm

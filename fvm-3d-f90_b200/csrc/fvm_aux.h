@@ -1,0 +1,39 @@
+// fvm_aux.h — launchers of the auxiliary kernels (fvm_aux.cu) and the
+// lookup of fused stage-kernel instantiations (fvm_stage_inst.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fvm_types.h"
+
+namespace fvm {
+
+cudaError_t launch_gather(double* base, int64_t vs, const int64_t* pairs, int64_t npairs, cudaStream_t s);
+cudaError_t launch_unpack(double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, const double* src,
+                          cudaStream_t s);
+cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, double* dst,
+                        int prim, double gm1, cudaStream_t s);
+cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* cases, DevCaseState* st, int ncases,
+                           unsigned long long* case_max, int role, cudaStream_t s);
+cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, DevCaseState* st, int ncases,
+                            const double* partials, int* counters, int ncounters, cudaStream_t s);
+cudaError_t launch_visc(const DevBlock* blocks, int nblocks, const DevCase* cases, int role, cudaStream_t s);
+
+// One compiled instantiation of the fused stage kernel.
+struct StageKernelInfo {
+  const void* fn = nullptr;
+  size_t smem = 0;
+  int threads = 0;
+  int tx = 0, ty = 0;
+};
+
+// Tile shapes compiled for every scheme (index -> TX x TY).
+constexpr int kNumTiles = 2;
+constexpr int kTileTX[kNumTiles] = {32, 16};
+constexpr int kTileTY[kNumTiles] = {8, 16};
+
+// prec: 0 exact FP64, 1 FP64, 2 FP32 flux; dim 2|3; recon 200..202;
+// flux 300|301|303; tb: textbook WENO (mirrored right state); tile 0..kNumTiles-1.
+bool lookup_stage_kernel(int prec, int dim, int recon, int flux, bool tb, int tile, StageKernelInfo* out);
+
+}  // namespace fvm

@@ -1,0 +1,1034 @@
+// fvm_engine.cu — host runtime of the B200 residual-and-update path and the
+// C ABI of include/fvm3d.h.
+//
+// The runtime owns device memory only; every entry point validates its
+// arguments on the host first (mirroring the reference's mpi%stop("Invalid
+// ...") checks, class_space_discret.f90:94-106, class_time_discret.f90:82-108)
+// and reports failures as status codes plus a message (ClassError's flag+info,
+// global_error.f90:18-33). No CUDA call is made before the first state upload
+// or step, so configuration errors surface without a GPU.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fvm_engine.h"
+
+namespace fvm {
+
+namespace {
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+inline int stage_roles(int S, int m, int* rin, int* rout) {
+  // RK3: A->B, (A,B)->C, (A,C)->A. RK4: A->B, B->C, C->B, B->A (q0 = A).
+  static const int r3[3][2] = {{ROLE_A, ROLE_B}, {ROLE_B, ROLE_C}, {ROLE_C, ROLE_A}};
+  static const int r4[4][2] = {{ROLE_A, ROLE_B}, {ROLE_B, ROLE_C}, {ROLE_C, ROLE_B}, {ROLE_B, ROLE_A}};
+  if (S == 3) {
+    *rin = r3[m - 1][0];
+    *rout = r3[m - 1][1];
+  } else {
+    *rin = r4[m - 1][0];
+    *rout = r4[m - 1][1];
+  }
+  return 0;
+}
+}  // namespace
+
+Engine::Engine() {}
+
+Engine::~Engine() {
+  release();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Engine::release() {
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  gexec_ = nullptr;
+  graph_ = nullptr;
+  for (auto& r : role_) {
+    if (r) cudaFree(r);
+    r = nullptr;
+  }
+  void* ptrs[] = {visc_, rhs_all_, d_blocks_, d_cases_, d_state_, d_tasks_, d_partials_, d_pairs_, d_counters_,
+                  d_casemax_, d_staging_};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  visc_ = rhs_all_ = nullptr;
+  d_blocks_ = nullptr;
+  d_cases_ = nullptr;
+  d_state_ = nullptr;
+  d_tasks_ = nullptr;
+  d_partials_ = nullptr;
+  d_pairs_ = nullptr;
+  d_counters_ = nullptr;
+  d_casemax_ = nullptr;
+  d_staging_ = nullptr;
+  for (auto& b : blocks) b.rhs_dev = nullptr;
+  planned_ = false;
+  prepared_ = false;
+}
+
+int Engine::cuda_fail(cudaError_t e, const char* where) {
+  return fail(FVM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                             \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);      \
+  } while (0)
+
+// ---------------------------------------------------------------- topology
+int Engine::add_case(const fvm_config& c) {
+  if (c.struct_size != (int32_t)sizeof(fvm_config)) return fail(FVM_ERR_INVALID, "fvm_config.struct_size mismatch");
+  if (c.idimension != 2 && c.idimension != 3) return fail(FVM_ERR_INVALID, "idimension must be 2 or 3");
+  if (c.equation != FVM_EQ_EULER && c.equation != FVM_EQ_NAVIER_STOKES)
+    return fail(FVM_ERR_INVALID, "Invalid equation type.");
+  if (c.reconstruct == FVM_RECON_WCNS)
+    return fail(FVM_ERR_UNSUPPORTED, "WCNS has no implementation in the reference");
+  if (c.reconstruct != FVM_RECON_SIMPLE && c.reconstruct != FVM_RECON_MUSCL && c.reconstruct != FVM_RECON_WENO)
+    return fail(FVM_ERR_INVALID, "Invalid reconstruct scheme.");
+  if (c.flux_split == FVM_FLUX_HLLC)
+    return fail(FVM_ERR_UNSUPPORTED, "HLLC has no implementation in the reference (its flux stays zero)");
+  if (c.flux_split != FVM_FLUX_ROE && c.flux_split != FVM_FLUX_VANLEER && c.flux_split != FVM_FLUX_AUSM)
+    return fail(FVM_ERR_INVALID, "Invalid flux split scheme.");
+  if (c.limiter != FVM_SCHEME_NULL && (c.limiter < FVM_LIMITER_NONE || c.limiter > FVM_LIMITER_VANALBADA))
+    return fail(FVM_ERR_INVALID, "Invalid limiter.");
+  if (c.time_scheme >= 102 && c.time_scheme <= 106)
+    return fail(FVM_ERR_UNSUPPORTED, "only Runge-Kutta time stepping exists in the reference");
+  if (c.time_scheme != FVM_TIME_RUNGE_KUTTA) return fail(FVM_ERR_INVALID, "Invalid time discretization scheme.");
+  if (c.rk_stages != 3 && c.rk_stages != 4) return fail(FVM_ERR_INVALID, "rk_stages must be 3 or 4");
+  if (c.timestep_set < FVM_DT_FIXED || c.timestep_set > FVM_DT_CFL_LOCAL)
+    return fail(FVM_ERR_INVALID, "Invalid timestep type.");
+  if (c.timestep_set == FVM_DT_FIXED && c.dt < -1.0E-6) return fail(FVM_ERR_INVALID, "Invalid time step.");
+  if (c.timestep_set != FVM_DT_FIXED && !(c.cfl > 0.0)) return fail(FVM_ERR_INVALID, "cfl must be positive");
+  if (c.compat != FVM_COMPAT_REFERENCE && c.compat != FVM_COMPAT_TEXTBOOK)
+    return fail(FVM_ERR_INVALID, "compat must be 0 or 1");
+  if (c.precision < FVM_PREC_FP64_EXACT || c.precision > FVM_PREC_FP32_FLUX)
+    return fail(FVM_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (!(c.gamma > 1.0)) return fail(FVM_ERR_INVALID, "gamma must exceed 1");
+  if (c.equation == FVM_EQ_NAVIER_STOKES && (!(c.mu >= 0.0) || !(c.prandtl > 0.0)))
+    return fail(FVM_ERR_INVALID, "Navier-Stokes needs mu >= 0 and prandtl > 0");
+  if (!cases.empty() && cases[0].cfg.rk_stages != c.rk_stages)
+    return fail(FVM_ERR_INVALID, "all cases of one engine share the RK stage count");
+  HCase hc;
+  hc.cfg = c;
+  cases.push_back(hc);
+  release();
+  return FVM_OK;
+}
+
+int Engine::add_block(int case_id, const int64_t n[3], const double dr[3], int* blk) {
+  if (case_id < 0 || case_id >= (int)cases.size()) return fail(FVM_ERR_INVALID, "bad case id");
+  if (!n || !dr) return fail(FVM_ERR_INVALID, "null nvert / dr");
+  for (int d = 0; d < 3; ++d) {
+    if (n[d] < 1 || n[d] > (1 << 20)) return fail(FVM_ERR_INVALID, "nvert out of range [1, 2^20]");
+    if (!(dr[d] > 0.0) || !std::isfinite(dr[d])) return fail(FVM_ERR_INVALID, "dr must be positive");
+  }
+  HBlock b;
+  b.case_id = case_id;
+  for (int d = 0; d < 3; ++d) {
+    b.n[d] = n[d];
+    b.dr[d] = dr[d];
+  }
+  blocks.push_back(b);
+  cases[case_id].blocks.push_back((int)blocks.size() - 1);
+  if (blk) *blk = (int)blocks.size() - 1;
+  release();
+  return FVM_OK;
+}
+
+int Engine::set_boundary(int blk, int region, int kind) {
+  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (region < 1 || region > 6) return fail(FVM_ERR_INVALID, "region must be 1..6");
+  HBlock& b = blocks[blk];
+  const int ax = (region - 1) / 2;
+  const bool hi = (region - 1) % 2 == 1;
+  const int idim = cases[b.case_id].cfg.idimension;
+  if (ax == 2 && idim == 2 && kind != FVM_BC_TRANSMISSIVE)
+    return fail(FVM_ERR_INVALID, "2D blocks have no k ghost regions to connect");
+  if (kind != FVM_BC_TRANSMISSIVE && kind != FVM_BC_PERIODIC && kind != FVM_BC_CONNECTED)
+    return fail(FVM_ERR_INVALID, "unknown boundary kind");
+  if (kind == FVM_BC_PERIODIC && b.n[ax] < kGhost)
+    return fail(FVM_ERR_INVALID, "periodic region needs at least 3 cells along its axis");
+  std::vector<HConn> keep;
+  for (auto& c : b.conns) {
+    const bool same = hi ? (c.range[ax][0] >= b.n[ax]) : (c.range[ax][1] < 0);
+    if (!same) keep.push_back(c);
+  }
+  b.conns = keep;
+  b.bc[region - 1] = kind;
+  if (kind == FVM_BC_PERIODIC) {
+    HConn c;
+    for (int d = 0; d < 3; ++d) {
+      c.range[d][0] = 0;
+      c.range[d][1] = b.n[d] - 1;
+      c.drange[d][0] = 0;
+      c.drange[d][1] = b.n[d] - 1;
+      c.dtype[d] = d + 1;
+    }
+    if (hi) {
+      c.range[ax][0] = b.n[ax];
+      c.range[ax][1] = b.n[ax] + 2;
+      c.drange[ax][0] = 0;
+      c.drange[ax][1] = 2;
+    } else {
+      c.range[ax][0] = -3;
+      c.range[ax][1] = -1;
+      c.drange[ax][0] = b.n[ax] - 3;
+      c.drange[ax][1] = b.n[ax] - 1;
+    }
+    c.donor = blk;
+    b.conns.push_back(c);
+  }
+  release();
+  return FVM_OK;
+}
+
+int Engine::connect(int blk, const int64_t range[3][2], int donor, const int64_t drange[3][2],
+                    const int32_t dtype[3]) {
+  if (blk < 0 || blk >= (int)blocks.size() || donor < 0 || donor >= (int)blocks.size())
+    return fail(FVM_ERR_INVALID, "bad block id");
+  if (!range || !drange || !dtype) return fail(FVM_ERR_INVALID, "null range");
+  int seen = 0;
+  for (int a = 0; a < 3; ++a) {
+    const int d = std::abs(dtype[a]);
+    if (d < 1 || d > 3) return fail(FVM_ERR_INVALID, "donor_type is not a signed permutation");
+    seen |= 1 << (d - 1);
+  }
+  if (seen != 7) return fail(FVM_ERR_INVALID, "donor_type is not a signed permutation");
+  HBlock& b = blocks[blk];
+  const HBlock& dn = blocks[donor];
+  if (dn.case_id != b.case_id) return fail(FVM_ERR_INVALID, "donor block belongs to another case");
+  HConn c;
+  c.donor = donor;
+  int out_axis = -1;
+  for (int a = 0; a < 3; ++a) {
+    c.range[a][0] = range[a][0];
+    c.range[a][1] = range[a][1];
+    c.drange[a][0] = drange[a][0];
+    c.drange[a][1] = drange[a][1];
+    c.dtype[a] = dtype[a];
+    if (c.range[a][1] < c.range[a][0]) return fail(FVM_ERR_INVALID, "empty range");
+    const int64_t s = dtype[a] > 0 ? 1 : -1;
+    if (c.drange[a][1] - c.drange[a][0] != s * (c.range[a][1] - c.range[a][0]))
+      return fail(FVM_ERR_INVALID, "donor range extent does not match");
+    const bool out = c.range[a][1] < 0 || c.range[a][0] >= b.n[a];
+    const bool in = c.range[a][0] >= 0 && c.range[a][1] < b.n[a];
+    if (out) {
+      if (out_axis >= 0) return fail(FVM_ERR_INVALID, "range is not a face ghost box");
+      out_axis = a;
+      if (c.range[a][0] < -kGhost || c.range[a][1] > b.n[a] + kGhost - 1)
+        return fail(FVM_ERR_INVALID, "range beyond the 3 ghost layers");
+    } else if (!in) {
+      return fail(FVM_ERR_INVALID, "range straddles the block boundary");
+    }
+  }
+  if (out_axis < 0) return fail(FVM_ERR_INVALID, "range holds no ghost cells");
+  if (out_axis == 2 && cases[b.case_id].cfg.idimension == 2)
+    return fail(FVM_ERR_INVALID, "2D blocks have no k ghost regions to connect");
+  for (int a = 0; a < 3; ++a) {
+    const int da = std::abs(dtype[a]) - 1;
+    for (int s = 0; s < 2; ++s)
+      if (c.drange[a][s] < 0 || c.drange[a][s] >= dn.n[da])
+        return fail(FVM_ERR_INVALID, "donor range outside the donor's real cells");
+  }
+  const int region = 2 * out_axis + (c.range[out_axis][0] >= b.n[out_axis] ? 2 : 1);
+  if (b.bc[region - 1] == FVM_BC_PERIODIC) {
+    // replacing the periodic self-connection of this region
+    std::vector<HConn> keep;
+    const bool hi = region % 2 == 0;
+    for (auto& e : b.conns) {
+      const bool same = hi ? (e.range[out_axis][0] >= b.n[out_axis]) : (e.range[out_axis][1] < 0);
+      if (!same) keep.push_back(e);
+    }
+    b.conns = keep;
+  }
+  b.bc[region - 1] = FVM_BC_CONNECTED;
+  b.conns.push_back(c);
+  release();
+  return FVM_OK;
+}
+
+int Engine::set_tuning(int case_id, int tile, int zchunk) {
+  if (case_id < 0 || case_id >= (int)cases.size()) return fail(FVM_ERR_INVALID, "bad case id");
+  if (tile < -1 || tile >= kNumTiles) return fail(FVM_ERR_INVALID, "bad tile index");
+  if (zchunk < 0) return fail(FVM_ERR_INVALID, "bad z chunk");
+  if (cases[case_id].tile == tile && cases[case_id].zchunk == zchunk) return FVM_OK;
+  cases[case_id].tile = tile;
+  cases[case_id].zchunk = zchunk;
+  if (!planned_) {
+    release();
+    return FVM_OK;
+  }
+  // re-plan keeping the state, time and residual history
+  std::vector<std::vector<double>> saved(blocks.size());
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    saved[b].resize(5 * blocks[b].n[0] * blocks[b].n[1] * blocks[b].n[2]);
+    int rc = get_state((int)b, saved[b].data(), 0);
+    if (rc) return rc;
+  }
+  std::vector<DevCaseState> st(cases.size());
+  CK(cudaMemcpyAsync(st.data(), d_state_, sizeof(DevCaseState) * cases.size(), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  int rc = plan();
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(d_state_, st.data(), sizeof(DevCaseState) * cases.size(), cudaMemcpyHostToDevice, stream));
+  for (size_t b = 0; b < blocks.size(); ++b) {
+    rc = set_state((int)b, saved[b].data());
+    if (rc) return rc;
+  }
+  return FVM_OK;
+}
+
+// Follow ghost rules until x is a real cell: the lowest out-of-range axis
+// first; transmissive clamps, connected maps through the connection whose
+// box holds x with the other axes clamped into the block.
+int Engine::resolve(int blk, int64_t x[3], int* out_blk) const {
+  for (int it = 0; it < 4; ++it) {
+    const HBlock& b = blocks[blk];
+    int a = -1;
+    for (int d = 0; d < 3 && a < 0; ++d)
+      if (x[d] < 0 || x[d] >= b.n[d]) a = d;
+    if (a < 0) {
+      *out_blk = blk;
+      return 0;
+    }
+    const bool hi = x[a] >= b.n[a];
+    const int region = 2 * a + (hi ? 2 : 1);
+    if (b.bc[region - 1] == FVM_BC_TRANSMISSIVE) {
+      x[a] = hi ? b.n[a] - 1 : 0;
+      continue;
+    }
+    int64_t xc[3] = {x[0], x[1], x[2]};
+    for (int d = 0; d < 3; ++d)
+      if (d != a) xc[d] = std::min<int64_t>(std::max<int64_t>(xc[d], 0), b.n[d] - 1);
+    const HConn* hit = nullptr;
+    for (const auto& c : b.conns) {
+      bool in = true;
+      for (int d = 0; d < 3; ++d) in = in && xc[d] >= c.range[d][0] && xc[d] <= c.range[d][1];
+      if (in) {
+        hit = &c;
+        break;
+      }
+    }
+    if (!hit) return -1;
+    int64_t y[3];
+    for (int d = 0; d < 3; ++d) {
+      const int dd = std::abs(hit->dtype[d]) - 1;
+      const int64_t s = hit->dtype[d] > 0 ? 1 : -1;
+      y[dd] = hit->drange[d][0] + s * (x[d] - hit->range[d][0]);
+    }
+    blk = hit->donor;
+    for (int d = 0; d < 3; ++d) x[d] = y[d];
+  }
+  return -1;
+}
+
+// ---------------------------------------------------------------- planning
+int Engine::ensure_planned() {
+  if (planned_) return FVM_OK;
+  return plan();
+}
+
+int Engine::plan() {
+  release();
+  if (cases.empty()) return fail(FVM_ERR_STATE, "no case configured");
+  if (blocks.empty()) return fail(FVM_ERR_STATE, "no block added");
+  if (!stream) {
+    CK(cudaGetDevice(&device));
+    CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  }
+  max_stages_ = cases[0].cfg.rk_stages;
+  nroles_ = (max_stages_ == 4) ? 4 : 3;
+  bool any_ns = false, any_rhs = false;
+  for (auto& c : cases) {
+    any_ns |= c.cfg.equation == FVM_EQ_NAVIER_STOKES;
+    any_rhs |= c.cfg.store_rhs != 0;
+  }
+
+  // -- coverage of connected regions
+  for (size_t bi = 0; bi < blocks.size(); ++bi) {
+    const HBlock& b = blocks[bi];
+    for (int region = 1; region <= 6; ++region) {
+      if (b.bc[region - 1] == FVM_BC_TRANSMISSIVE) continue;
+      const int ax = (region - 1) / 2;
+      const bool hi = (region - 1) % 2 == 1;
+      const int t1 = ax == 0 ? 1 : 0, t2 = ax == 2 ? 1 : 2;
+      std::vector<char> cov((size_t)3 * b.n[t1] * b.n[t2], 0);
+      for (const auto& c : b.conns) {
+        const bool same = hi ? (c.range[ax][0] >= b.n[ax]) : (c.range[ax][1] < 0);
+        if (!same) continue;
+        for (int64_t l = c.range[ax][0]; l <= c.range[ax][1]; ++l)
+          for (int64_t u = c.range[t1][0]; u <= c.range[t1][1]; ++u)
+            for (int64_t w = c.range[t2][0]; w <= c.range[t2][1]; ++w) {
+              const int64_t layer = hi ? l - b.n[ax] : -1 - l;
+              cov[(size_t)(layer * b.n[t1] + u) * b.n[t2] + w] = 1;
+            }
+      }
+      for (char v : cov)
+        if (!v) {
+          char m[160];
+          std::snprintf(m, sizeof m, "region %d of block %zu is connected but not every ghost cell has a donor",
+                        region, bi);
+          return fail(FVM_ERR_INVALID, m);
+        }
+    }
+  }
+
+  // -- layout
+  int64_t off = 0;
+  size_t max_cells = 0;
+  for (auto& b : blocks) {
+    const int idim = cases[b.case_id].cfg.idimension;
+    b.px = round_up(b.n[0] + kPadX + kGhost, 4);
+    b.py = b.n[1] + 2 * kGhost;
+    b.zpad = (idim == 3) ? kGhost : 0;
+    b.pz = b.n[2] + 2 * b.zpad;
+    b.sy = b.px;
+    b.sz = b.px * b.py;
+    b.org = kPadX + kGhost * b.sy + b.zpad * b.sz;
+    b.slab_off = off;
+    off = round_up(off + b.px * b.py * b.pz, 64);
+    max_cells = std::max(max_cells, (size_t)(b.n[0] * b.n[1] * b.n[2]));
+  }
+  cap_ = round_up(off, 64);
+  if (cap_ >= ((int64_t)1 << 40)) return fail(FVM_ERR_INVALID, "grid too large");
+  for (int r = 0; r < nroles_; ++r) {
+    cudaError_t e = cudaMalloc(&role_[r], sizeof(double) * 5 * cap_);
+    if (e != cudaSuccess) return fail(FVM_ERR_NOMEM, std::string("state allocation: ") + cudaGetErrorString(e));
+    CK(cudaMemsetAsync(role_[r], 0, sizeof(double) * 5 * cap_, stream));
+  }
+  for (int r = nroles_; r < NROLE; ++r) role_[r] = role_[ROLE_A];
+  if (any_ns) {
+    CK(cudaMalloc(&visc_, sizeof(double) * 5 * cap_));
+    CK(cudaMemsetAsync(visc_, 0, sizeof(double) * 5 * cap_, stream));
+  }
+  if (any_rhs) {
+    int64_t tot = 0;
+    for (auto& b : blocks)
+      if (cases[b.case_id].cfg.store_rhs) tot += 5 * b.n[0] * b.n[1] * b.n[2];
+    CK(cudaMalloc(&rhs_all_, sizeof(double) * tot));
+    CK(cudaMemsetAsync(rhs_all_, 0, sizeof(double) * tot, stream));
+    int64_t o = 0;
+    for (auto& b : blocks)
+      if (cases[b.case_id].cfg.store_rhs) {
+        b.rhs_dev = rhs_all_ + o;
+        o += 5 * b.n[0] * b.n[1] * b.n[2];
+      }
+  }
+  staging_bytes_ = sizeof(double) * 5 * max_cells;
+  CK(cudaMalloc(&d_staging_, staging_bytes_));
+
+  // -- groups (one per distinct kernel) and tasks
+  groups.clear();
+  std::vector<Task> tasks;
+  std::vector<int> block_task0(blocks.size()), block_ntask(blocks.size());
+  for (size_t ci = 0; ci < cases.size(); ++ci) {
+    HCase& hc = cases[ci];
+    const fvm_config& c = hc.cfg;
+    const int dim = c.idimension;
+    const int prec = c.precision;
+    const bool tb = c.reconstruct == FVM_RECON_WENO && c.compat == FVM_COMPAT_TEXTBOOK;
+    int tile = hc.tile;
+    if (tile < 0) {
+      // heuristic: 32 x 8 when the blocks are at least 32 wide, else 16 x 16
+      int64_t minx = 1 << 30;
+      for (int b : hc.blocks) minx = std::min(minx, blocks[b].n[0]);
+      tile = (minx >= 32) ? 0 : 1;
+    }
+    int gi = -1;
+    for (size_t g = 0; g < groups.size(); ++g) {
+      const Group& G = groups[g];
+      if (G.prec == prec && G.dim == dim && G.recon == c.reconstruct && G.flux == c.flux_split && G.tb == tb &&
+          G.tile == tile)
+        gi = (int)g;
+    }
+    if (gi < 0) {
+      Group G;
+      G.prec = prec;
+      G.dim = dim;
+      G.recon = c.reconstruct;
+      G.flux = c.flux_split;
+      G.tb = tb;
+      G.tile = tile;
+      if (!lookup_stage_kernel(prec, dim, c.reconstruct, c.flux_split, tb, tile, &G.k))
+        return fail(FVM_ERR_UNSUPPORTED, "no compiled stage kernel for this scheme combination");
+      groups.push_back(G);
+      gi = (int)groups.size() - 1;
+    }
+    hc.group = gi;
+  }
+  // occupancy per group
+  for (auto& G : groups) {
+    CK(cudaFuncSetAttribute(G.k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.k.smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, G.k.fn, G.k.threads, G.k.smem));
+    if (occ < 1) return fail(FVM_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
+    G.grid = occ * num_sms;
+  }
+  // tasks grouped by kernel, blocks contiguous inside a group
+  for (size_t g = 0; g < groups.size(); ++g) {
+    Group& G = groups[g];
+    G.task_off = (int)tasks.size();
+    // total tile columns of the group for the z-chunk heuristic
+    int64_t cols_planes = 0;
+    for (auto& hc : cases)
+      if (hc.group == (int)g)
+        for (int bi : hc.blocks) {
+          const HBlock& b = blocks[bi];
+          cols_planes += ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty) * b.n[2];
+        }
+    for (auto& hc : cases) {
+      if (hc.group != (int)g) continue;
+      int64_t L = hc.zchunk;
+      if (G.dim == 3 && L <= 0) {
+        L = (cols_planes + 3 * (int64_t)G.grid - 1) / (3 * (int64_t)G.grid);
+        L = std::max<int64_t>(8, round_up(L, 4));
+      }
+      for (int bi : hc.blocks) {
+        HBlock& b = blocks[bi];
+        block_task0[bi] = (int)tasks.size();
+        const int64_t Lb = (G.dim == 3) ? std::min<int64_t>(L, b.n[2]) : b.n[2];
+        for (int64_t z0 = 0; z0 < b.n[2]; z0 += Lb)
+          for (int64_t y0 = 0; y0 < b.n[1]; y0 += G.k.ty)
+            for (int64_t x0 = 0; x0 < b.n[0]; x0 += G.k.tx) {
+              Task t;
+              t.blk = bi;
+              t.x0 = (int)x0;
+              t.y0 = (int)y0;
+              t.z0 = (int)z0;
+              t.z1 = (int)std::min<int64_t>(z0 + Lb, b.n[2]);
+              t.slot = (int)tasks.size();
+              tasks.push_back(t);
+            }
+        block_ntask[bi] = (int)tasks.size() - block_task0[bi];
+      }
+    }
+    G.ntasks = (int)tasks.size() - G.task_off;
+    G.grid = std::max(1, std::min(G.grid, G.ntasks));
+  }
+  ntasks_total = (int64_t)tasks.size();
+
+  // -- ghost gather pairs (slab element offsets)
+  std::vector<int64_t> pairs;
+  auto add_pair = [&](int bi, const int64_t x[3]) -> int {
+    int64_t y[3] = {x[0], x[1], x[2]};
+    int src_blk = -1;
+    if (resolve(bi, y, &src_blk) != 0) return -1;
+    const HBlock& b = blocks[bi];
+    const HBlock& s = blocks[src_blk];
+    pairs.push_back(b.slab_off + b.org + x[0] + x[1] * b.sy + x[2] * b.sz);
+    pairs.push_back(s.slab_off + s.org + y[0] + y[1] * s.sy + y[2] * s.sz);
+    return 0;
+  };
+  for (size_t bi = 0; bi < blocks.size(); ++bi) {
+    const HBlock& b = blocks[bi];
+    for (const auto& c : b.conns)
+      for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
+        for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j)
+          for (int64_t i = c.range[0][0]; i <= c.range[0][1]; ++i) {
+            const int64_t x[3] = {i, j, k};
+            if (add_pair((int)bi, x) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
+          }
+    if (cases[b.case_id].cfg.equation == FVM_EQ_NAVIER_STOKES) {
+      // layer-1 edge ghosts read by the viscous stencil where both regions are
+      // connected (a transmissive axis is clamped on load instead)
+      const int idim = cases[b.case_id].cfg.idimension;
+      for (int a = 0; a < idim; ++a)
+        for (int a2 = a + 1; a2 < idim; ++a2) {
+          const int c3 = 3 - a - a2;
+          for (int sa = 0; sa < 2; ++sa)
+            for (int sb = 0; sb < 2; ++sb) {
+              if (b.bc[2 * a + sa] == FVM_BC_TRANSMISSIVE || b.bc[2 * a2 + sb] == FVM_BC_TRANSMISSIVE) continue;
+              for (int64_t t = 0; t < b.n[c3]; ++t) {
+                int64_t x[3];
+                x[a] = sa ? b.n[a] : -1;
+                x[a2] = sb ? b.n[a2] : -1;
+                x[c3] = t;
+                if (add_pair((int)bi, x) != 0) return fail(FVM_ERR_INVALID, "edge ghost without a real donor");
+              }
+            }
+        }
+    }
+  }
+  npairs = (int64_t)pairs.size() / 2;
+
+  // -- device descriptors
+  h_dblocks_.assign(blocks.size(), DevBlock());
+  for (size_t bi = 0; bi < blocks.size(); ++bi) {
+    const HBlock& b = blocks[bi];
+    DevBlock& d = h_dblocks_[bi];
+    std::memset(&d, 0, sizeof d);
+    for (int r = 0; r < NROLE; ++r) d.q[r] = role_[r] + b.slab_off + b.org;
+    d.rhs = b.rhs_dev;
+    d.visc = (visc_ && cases[b.case_id].cfg.equation == FVM_EQ_NAVIER_STOKES) ? visc_ + b.slab_off + b.org : nullptr;
+    d.vs = cap_;
+    for (int a = 0; a < 3; ++a) {
+      d.n[a] = (int32_t)b.n[a];
+      d.dr[a] = b.dr[a];
+      d.inv_dr[a] = 1.0 / b.dr[a];
+    }
+    d.sy = (int32_t)b.sy;
+    d.sz = (int32_t)b.sz;
+    int mask = 0;
+    for (int r = 0; r < 6; ++r)
+      if (b.bc[r] != FVM_BC_TRANSMISSIVE) mask |= 1 << r;
+    d.ghost_mask = mask;
+    d.case_id = b.case_id;
+    d.task0 = block_task0[bi];
+    d.ntask = block_ntask[bi];
+  }
+  std::vector<DevCase> hcases(cases.size());
+  std::vector<DevCaseState> hstate(cases.size());
+  int b0 = 0;
+  for (size_t ci = 0; ci < cases.size(); ++ci) {
+    const fvm_config& c = cases[ci].cfg;
+    DevCase& d = hcases[ci];
+    std::memset(&d, 0, sizeof d);
+    d.gamma = c.gamma;
+    d.gm1 = c.gamma - 1.0;
+    d.kappa = c.kappa;
+    d.entropy_fix = c.entropy_fix;
+    d.cfl = c.cfl;
+    d.dt_fixed = c.dt;
+    d.mu = c.mu;
+    d.prandtl = c.prandtl;
+    d.kq = c.mu * c.gamma / (c.prandtl * (c.gamma - 1.0));
+    d.limiter = c.limiter;
+    d.compat = c.compat;
+    d.timestep_set = c.timestep_set;
+    d.idim = c.idimension;
+    d.rk_stages = c.rk_stages;
+    d.equation = c.equation;
+    d.store_rhs = c.store_rhs;
+    // blocks of a case are contiguous in creation order only if added so;
+    // the finalize walks [block0, block0+nblocks), so require it.
+    d.block0 = cases[ci].blocks.empty() ? 0 : cases[ci].blocks.front();
+    d.nblocks = (int)cases[ci].blocks.size();
+    for (int k = 0; k < d.nblocks; ++k)
+      if (cases[ci].blocks[k] != d.block0 + k) return fail(FVM_ERR_INVALID, "blocks of a case must be added contiguously");
+    b0 += d.nblocks;
+    std::memset(&hstate[ci], 0, sizeof(DevCaseState));
+    hstate[ci].dt = c.dt;
+  }
+  (void)b0;
+  CK(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks.size()));
+  CK(cudaMalloc(&d_cases_, sizeof(DevCase) * cases.size()));
+  CK(cudaMalloc(&d_state_, sizeof(DevCaseState) * cases.size()));
+  CK(cudaMalloc(&d_tasks_, sizeof(Task) * std::max<size_t>(1, tasks.size())));
+  CK(cudaMalloc(&d_partials_, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size())));
+  CK(cudaMalloc(&d_pairs_, sizeof(int64_t) * std::max<size_t>(2, pairs.size())));
+  ncounters_ = max_stages_ * (int)groups.size();
+  CK(cudaMalloc(&d_counters_, sizeof(int) * std::max(1, ncounters_)));
+  CK(cudaMalloc(&d_casemax_, sizeof(unsigned long long) * cases.size()));
+  CK(cudaMemcpyAsync(d_blocks_, h_dblocks_.data(), sizeof(DevBlock) * blocks.size(), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_cases_, hcases.data(), sizeof(DevCase) * cases.size(), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(d_state_, hstate.data(), sizeof(DevCaseState) * cases.size(), cudaMemcpyHostToDevice, stream));
+  if (!tasks.empty())
+    CK(cudaMemcpyAsync(d_tasks_, tasks.data(), sizeof(Task) * tasks.size(), cudaMemcpyHostToDevice, stream));
+  if (!pairs.empty())
+    CK(cudaMemcpyAsync(d_pairs_, pairs.data(), sizeof(int64_t) * pairs.size(), cudaMemcpyHostToDevice, stream));
+  CK(cudaMemsetAsync(d_counters_, 0, sizeof(int) * std::max(1, ncounters_), stream));
+  CK(cudaMemsetAsync(d_partials_, 0, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size()), stream));
+  CK(cudaStreamSynchronize(stream));
+  planned_ = true;
+  prepared_ = false;
+  return build_graph();
+}
+
+// Enqueue one full time step on `stream`: per stage the optional viscous
+// kernel, one fused stage launch per scheme group and the ghost gather; then
+// the finalize. With `evs`, an event is recorded after every launch and the
+// kind of each launch (1 stage, 2 gather, 3 viscous, 4 finalize) returned.
+int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
+  bool any_ns = false;
+  for (auto& c : cases) any_ns |= c.cfg.equation == FVM_EQ_NAVIER_STOKES;
+  const int S = max_stages_;
+  int n = 0;
+  auto mark = [&](int kind) -> cudaError_t {
+    if (evs && n < nev) {
+      kinds[n] = kind;
+      cudaError_t e = cudaEventRecord(evs[n + 1], stream);
+      ++n;
+      return e;
+    }
+    ++n;
+    return cudaSuccess;
+  };
+  if (evs && nev > 0) CK(cudaEventRecord(evs[0], stream));
+  for (int m = 1; m <= S; ++m) {
+    int rin, rout;
+    stage_roles(S, m, &rin, &rout);
+    if (any_ns) {
+      CK(launch_visc(d_blocks_, (int)blocks.size(), d_cases_, rin, stream));
+      CK(mark(3));
+    }
+    for (size_t g = 0; g < groups.size(); ++g) {
+      const Group& G = groups[g];
+      StageArgs a;
+      a.tasks = d_tasks_ + G.task_off;
+      a.ntasks = G.ntasks;
+      a.counter = d_counters_ + (m - 1) * (int)groups.size() + (int)g;
+      a.blocks = d_blocks_;
+      a.cases = d_cases_;
+      a.cstate = d_state_;
+      a.partials = d_partials_;
+      a.m = m;
+      a.rin = rin;
+      a.rout = rout;
+      a.rq0 = ROLE_A;
+      a.racc = (S == 4) ? ROLE_ACC : ROLE_A;
+      a.last = (m == S) ? 1 : 0;
+      void* args[] = {&a};
+      CK(cudaLaunchKernel(G.k.fn, dim3(G.grid), dim3(G.k.threads), args, G.k.smem, stream));
+      CK(mark(1));
+    }
+    if (npairs > 0) {
+      CK(launch_gather(role_[rout], cap_, d_pairs_, npairs, stream));
+      CK(mark(2));
+    }
+  }
+  CK(launch_finalize(d_blocks_, d_cases_, d_state_, (int)cases.size(), d_partials_, d_counters_, ncounters_, stream));
+  CK(mark(4));
+  if (nlaunch) *nlaunch = n;
+  return FVM_OK;
+}
+
+int Engine::build_graph() {
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  gexec_ = nullptr;
+  graph_ = nullptr;
+  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  int launches = 0;
+  int rc = enqueue_step(nullptr, 0, nullptr, &launches);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+  graph_ = g;
+  CK(cudaGraphInstantiate(&gexec_, graph_, 0));
+  kernel_launches_per_step = launches;
+  return FVM_OK;
+}
+
+int Engine::profile_step(float* ms, int* kinds, int cap, int* n) {
+  int rc = ensure_planned();
+  if (rc) return rc;
+  if (!prepared_) {
+    rc = prepare();
+    if (rc) return rc;
+  }
+  const int nev = kernel_launches_per_step + 1;
+  std::vector<cudaEvent_t> ev(nev);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<int> k(nev, 0);
+  int nl = 0;
+  rc = enqueue_step(ev.data(), nev - 1, k.data(), &nl);
+  if (rc) return rc;
+  CK(cudaEventSynchronize(ev[nev - 1]));
+  const int m = std::min(cap, nl);
+  for (int i = 0; i < m; ++i) {
+    CK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+    kinds[i] = k[i];
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  *n = m;
+  return FVM_OK;
+}
+
+int Engine::prepare() {
+  int rc = ensure_planned();
+  if (rc) return rc;
+  if (npairs > 0) CK(launch_gather(role_[ROLE_A], cap_, d_pairs_, npairs, stream));
+  CK(launch_init_dt(d_blocks_, (int)blocks.size(), d_cases_, d_state_, (int)cases.size(), d_casemax_, ROLE_A,
+                    stream));
+  prepared_ = true;
+  return FVM_OK;
+}
+
+// ---------------------------------------------------------------- state
+int Engine::set_state(int blk, const double* q) {
+  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!q) return fail(FVM_ERR_INVALID, "null state");
+  int rc = ensure_planned();
+  if (rc) return rc;
+  const HBlock& b = blocks[blk];
+  const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
+  CK(cudaMemcpyAsync(d_staging_, q, bytes, cudaMemcpyHostToDevice, stream));
+  CK(launch_unpack(h_dblocks_[blk].q[ROLE_A], cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
+                   d_staging_, stream));
+  CK(cudaStreamSynchronize(stream));
+  prepared_ = false;
+  return FVM_OK;
+}
+
+int Engine::get_state(int blk, double* q, int prim) {
+  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!q) return fail(FVM_ERR_INVALID, "null output");
+  if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
+  const HBlock& b = blocks[blk];
+  const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
+  CK(launch_pack(h_dblocks_[blk].q[ROLE_A], cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
+                 d_staging_, prim, cases[b.case_id].cfg.gamma - 1.0, stream));
+  CK(cudaMemcpyAsync(q, d_staging_, bytes, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  return FVM_OK;
+}
+
+int Engine::get_rhs(int blk, double* rhs) {
+  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!rhs) return fail(FVM_ERR_INVALID, "null output");
+  const HBlock& b = blocks[blk];
+  if (!cases[b.case_id].cfg.store_rhs) return fail(FVM_ERR_STATE, "store_rhs is off");
+  if (!planned_ || !b.rhs_dev) return fail(FVM_ERR_STATE, "no step taken yet");
+  const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
+  CK(cudaMemcpyAsync(rhs, b.rhs_dev, bytes, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  return FVM_OK;
+}
+
+int Engine::step(int nsteps) {
+  if (nsteps < 0) return fail(FVM_ERR_INVALID, "nsteps < 0");
+  if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
+  if (!prepared_) {
+    int rc = prepare();
+    if (rc) return rc;
+  }
+  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(gexec_, stream));
+  return FVM_OK;
+}
+
+int Engine::read_case_state(int case_id, DevCaseState* out) {
+  if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
+  CK(cudaMemcpyAsync(out, d_state_ + case_id, sizeof(DevCaseState), cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  return FVM_OK;
+}
+
+int Engine::time_stage(int reps, float* ms) {
+  int rc = ensure_planned();
+  if (rc) return rc;
+  if (!prepared_) {
+    rc = prepare();
+    if (rc) return rc;
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, stream));
+  for (int i = 0; i < reps; ++i) CK(cudaGraphLaunch(gexec_, stream));
+  CK(cudaEventRecord(e1, stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms /= (float)std::max(1, reps);
+  return FVM_OK;
+}
+
+}  // namespace fvm
+
+// ====================================================================== C ABI
+struct fvm_ctx {
+  fvm::Engine eng;
+  int case_id = 0;
+};
+
+static std::string g_create_error;
+
+extern "C" {
+
+int fvm_abi_version(void) { return FVM3D_ABI_VERSION; }
+
+int fvm_config_default(fvm_config* c) {
+  if (!c) return FVM_ERR_INVALID;
+  std::memset(c, 0, sizeof *c);
+  c->struct_size = (int32_t)sizeof(fvm_config);
+  c->idimension = 3;
+  c->equation = FVM_EQ_EULER;
+  c->reconstruct = FVM_RECON_MUSCL;
+  c->limiter = FVM_SCHEME_NULL;
+  c->flux_split = FVM_FLUX_ROE;
+  c->time_scheme = FVM_TIME_RUNGE_KUTTA;
+  c->rk_stages = 3;
+  c->timestep_set = FVM_DT_FIXED;
+  c->compat = FVM_COMPAT_REFERENCE;
+  c->precision = FVM_PREC_FP64_EXACT;
+  c->store_rhs = 0;
+  c->kappa = -1.0;       // ClassSpaceDiscret%kappa default (class_space_discret.f90:29)
+  c->entropy_fix = 0.05; // ClassSpaceDiscret%entropy_fix_coeff (class_space_discret.f90:32)
+  c->gamma = 1.4;        // ClassFlowField%gamma (class_flow_field.f90:41)
+  c->dt = 0.0;
+  c->cfl = 0.5;
+  c->mu = 0.0;
+  c->prandtl = 0.71;
+  return FVM_OK;
+}
+
+int fvm_create(const fvm_config* cfg, fvm_ctx** out) {
+  if (!cfg || !out) {
+    g_create_error = "null argument";
+    return FVM_ERR_INVALID;
+  }
+  *out = nullptr;
+  fvm_ctx* c = new (std::nothrow) fvm_ctx();
+  if (!c) return FVM_ERR_NOMEM;
+  int rc = c->eng.add_case(*cfg);
+  if (rc) {
+    g_create_error = c->eng.err;
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return FVM_OK;
+}
+
+int fvm_add_block(fvm_ctx* ctx, const int64_t nvert[3], const double dr[3], int* blk) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.add_block(ctx->case_id, nvert, dr, blk);
+}
+
+int fvm_set_boundary(fvm_ctx* ctx, int blk, int region, int kind) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.set_boundary(blk, region, kind);
+}
+
+int fvm_connect(fvm_ctx* ctx, int blk, const int64_t range[3][2], int donor, const int64_t donor_range[3][2],
+                const int32_t donor_type[3]) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.connect(blk, range, donor, donor_range, donor_type);
+}
+
+int fvm_set_state(fvm_ctx* ctx, int blk, const double* q) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.set_state(blk, q);
+}
+
+int fvm_get_state(fvm_ctx* ctx, int blk, double* q) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.get_state(blk, q, 0);
+}
+
+int fvm_get_primitive(fvm_ctx* ctx, int blk, double* p) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.get_state(blk, p, 1);
+}
+
+int fvm_get_rhs(fvm_ctx* ctx, int blk, double* rhs) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.get_rhs(blk, rhs);
+}
+
+int fvm_step(fvm_ctx* ctx, int nsteps, double* t, double* res_abs, double* res_rel) {
+  if (!ctx) return FVM_ERR_INVALID;
+  int rc = ctx->eng.step(nsteps);
+  if (rc) return rc;
+  fvm::DevCaseState s;
+  rc = ctx->eng.read_case_state(ctx->case_id, &s);
+  if (rc) return rc;
+  if (t) *t = s.t;
+  if (res_abs) std::memcpy(res_abs, s.res_abs, sizeof s.res_abs);
+  if (res_rel) std::memcpy(res_rel, s.res_rel, sizeof s.res_rel);
+  if (s.status == FVM_ERR_NONFINITE) return ctx->eng.fail(FVM_ERR_NONFINITE, "Error: ABSRES NaN");
+  if (s.status == FVM_ERR_DIVERGED)
+    return ctx->eng.fail(FVM_ERR_DIVERGED, "Error: Absolute Residual Exceeds Threshold 1E10.");
+  return FVM_OK;
+}
+
+int fvm_run(fvm_ctx* ctx, int64_t max_step, double total_time, double absolute_residual, double relative_residual,
+            int64_t* steps_done, int* reason) {
+  if (!ctx) return FVM_ERR_INVALID;
+  if (absolute_residual < 0.0) return ctx->eng.fail(FVM_ERR_INVALID, "Invalid minimum absolute residual.");
+  if (relative_residual < 0.0) return ctx->eng.fail(FVM_ERR_INVALID, "Invalid minimum relative residual.");
+  if (total_time < -1.0E-6) return ctx->eng.fail(FVM_ERR_INVALID, "Invalid total time.");
+  const double time_tol = 1.0E-10;  // class_iteration.f90 (file-local 239)
+  int64_t done = 0;
+  int why = FVM_STOP_NONE;
+  fvm::DevCaseState s;
+  std::memset(&s, 0, sizeof s);
+  for (;;) {
+    // converged() (class_iteration.f90, file-local 145-192)
+    if (s.step != 0) {
+      if (s.step == max_step) why = FVM_STOP_MAX_STEP;
+      else if (s.t > total_time - time_tol) why = FVM_STOP_MAX_TIME;
+      else if (s.res_abs[5] < absolute_residual) why = FVM_STOP_ABS_RESIDUAL;
+      else if (s.res_rel[5] < relative_residual) why = FVM_STOP_REL_RESIDUAL;
+      else if (s.res_abs[5] > 1.0E10) {
+        if (steps_done) *steps_done = done;
+        return ctx->eng.fail(FVM_ERR_DIVERGED, "Error: Absolute Residual Exceeds Threshold 1E10.");
+      } else if (std::isnan(s.res_abs[5])) {
+        if (steps_done) *steps_done = done;
+        return ctx->eng.fail(FVM_ERR_NONFINITE, "Error: ABSRES NaN");
+      }
+      if (why != FVM_STOP_NONE) break;
+    }
+    int rc = ctx->eng.step(1);
+    if (rc) return rc;
+    rc = ctx->eng.read_case_state(ctx->case_id, &s);
+    if (rc) return rc;
+    ++done;
+  }
+  if (steps_done) *steps_done = done;
+  if (reason) *reason = why;
+  return FVM_OK;
+}
+
+int fvm_get_time(fvm_ctx* ctx, double* t, double* dt, int64_t* step) {
+  if (!ctx) return FVM_ERR_INVALID;
+  fvm::DevCaseState s;
+  std::memset(&s, 0, sizeof s);
+  int rc = ctx->eng.read_case_state(ctx->case_id, &s);
+  if (rc) return rc;
+  if (t) *t = s.t;
+  if (dt) *dt = s.dt_last;
+  if (step) *step = s.step;
+  return FVM_OK;
+}
+
+int fvm_last_error(const fvm_ctx* ctx, char* buf, size_t n) {
+  if (!buf || n == 0) return FVM_ERR_INVALID;
+  const std::string& m = ctx ? ctx->eng.err : g_create_error;
+  std::snprintf(buf, n, "%s", m.c_str());
+  return FVM_OK;
+}
+
+int fvm_tune_set(fvm_ctx* ctx, int case_id, int tile, int zchunk) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.set_tuning(case_id, tile, zchunk);
+}
+
+int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step) {
+  if (!ctx || !ms_per_step || reps < 1) return FVM_ERR_INVALID;
+  return ctx->eng.time_stage(reps, ms_per_step);
+}
+
+int fvm_profile_step(fvm_ctx* ctx, float* ms, int32_t* kinds, int cap, int* n) {
+  if (!ctx || !ms || !kinds || !n || cap < 1) return FVM_ERR_INVALID;
+  std::vector<int> k(cap);
+  int rc = ctx->eng.profile_step(ms, k.data(), cap, n);
+  for (int i = 0; i < *n; ++i) kinds[i] = k[i];
+  return rc;
+}
+
+int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n) {
+  if (!ctx || !n) return FVM_ERR_INVALID;
+  int rc = ctx->eng.ensure_planned();
+  if (rc) return rc;
+  *n = ctx->eng.kernel_launches_per_step;
+  return FVM_OK;
+}
+
+int fvm_destroy(fvm_ctx* ctx) {
+  delete ctx;
+  return FVM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,358 @@
+// fvm_schemes.cuh — point-wise reconstruction and flux functions of the fused
+// sweep, templated on the arithmetic type R and on EX (exact mode).
+//
+// EX = true reproduces the reference's expression trees operation by
+// operation (the translation unit is compiled with -fmad=false), so results
+// are bit-identical to the CPU oracle. EX = false keeps the same mathematics
+// but shares reciprocals, uses the division-free WENO weights and lets the
+// compiler contract to FMA.
+//
+// The face normal is always an axis vector (class_space_discret.f90:458-461),
+// so every term multiplied by a zero normal component is dropped: x + y*0 and
+// x - y*0 equal x as numbers (only the sign of a zero can differ), and x*1 is
+// exact. DIR is the sweep axis 0..2.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fvm {
+
+enum ReconId { RECON_SIMPLE_ = 200, RECON_MUSCL_ = 201, RECON_WENO_ = 202 };
+enum FluxId { FLUX_ROE_ = 300, FLUX_VANLEER_ = 301, FLUX_AUSM_ = 303 };
+enum LimiterId { LIM_NONE_ = 250, LIM_MINMOD_ = 251, LIM_VANLEER_ = 252, LIM_VANALBADA_ = 253 };
+enum PrecId { PREC_EXACT = 0, PREC_FP64 = 1, PREC_FP32 = 2 };
+
+template <int P> struct PrecT { using R = double; static constexpr bool ex = true; };
+template <> struct PrecT<PREC_FP64> { using R = double; static constexpr bool ex = false; };
+template <> struct PrecT<PREC_FP32> { using R = float; static constexpr bool ex = false; };
+
+template <class R> struct Prim5 { R r, u, v, w, p; };
+
+// Case constants in the arithmetic type of the sweep.
+template <class R> struct SchemeConst {
+  R gamma, gm1, goverg1, two_g2m1, fix, kappa, omk, opk;
+  int limiter;
+  int textbook;
+};
+
+__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
+__device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double abs_(double x) { return fabs(x); }
+__device__ __forceinline__ float abs_(float x) { return fabsf(x); }
+__device__ __forceinline__ double sgn1_(double x) { return copysign(1.0, x); }
+__device__ __forceinline__ float sgn1_(float x) { return copysignf(1.0f, x); }
+template <class R> __device__ __forceinline__ R min2_(R a, R b) { return (b < a) ? b : a; }
+
+template <int DIR, class R> __device__ __forceinline__ R nrm_(R u, R v, R w) {
+  return DIR == 0 ? u : (DIR == 1 ? v : w);
+}
+
+// ------------------------------------------------------------ q -> p
+// convert_q_to_p_* (class_flow_field.f90:383-444)
+template <class R, bool EX>
+__device__ __forceinline__ Prim5<R> cons2prim(R q0, R q1, R q2, R q3, R q4, R gm1) {
+  Prim5<R> s;
+  s.r = q0;
+  if constexpr (EX) {
+    s.u = q1 / q0;
+    s.v = q2 / q0;
+    s.w = q3 / q0;
+    s.p = gm1 * (q4 - R(0.5) * q0 * (s.u * s.u + s.v * s.v + s.w * s.w));
+  } else {
+    const R ir = rcp_(q0);
+    s.u = q1 * ir;
+    s.v = q2 * ir;
+    s.w = q3 * ir;
+    s.p = gm1 * (q4 - R(0.5) * (q1 * s.u + q2 * s.v + q3 * s.w));
+  }
+  return s;
+}
+
+// ------------------------------------------------------------ MUSCL
+// scheme_reconstruct_MUSCL.f90:114-226. Limited differences of the centre
+// p2 of the stencil (p1, p2, p3).
+template <class R>
+__device__ __forceinline__ void muscl_slopes(R p1, R p2, R p3, int lim, R& Dbm, R& Dbp) {
+  const R Dm = p2 - p1;
+  const R Dp = p3 - p2;
+  if (lim == LIM_MINMOD_) {
+    // minmod(x, y, b=1) = 0.5*(sign(x)+sign(y))*min(|x|,|b*y|)
+    Dbm = R(0.5) * (sgn1_(Dm) + sgn1_(Dp)) * min2_(abs_(Dm), abs_(Dp));
+    Dbp = R(0.5) * (sgn1_(Dp) + sgn1_(Dm)) * min2_(abs_(Dp), abs_(Dm));
+  } else if (lim == LIM_VANLEER_) {
+    Dbm = (sgn1_(Dm) + sgn1_(Dp)) * Dm * Dp / (abs_(Dm) + abs_(Dp) + R(1.0E-6));
+    Dbp = Dbm;
+  } else if (lim == LIM_VANALBADA_) {
+    Dbm = (Dm * (Dp * Dp + R(1.0E-6)) + Dp * (Dm * Dm + R(1.0E-6))) / (Dm * Dm + Dp * Dp + R(1.0E-6));
+    Dbp = Dbm;
+  } else {  // none_ / NULL
+    Dbm = Dm;
+    Dbp = Dp;
+  }
+}
+// wind = -1: left state of the face right of p2.
+template <class R>
+__device__ __forceinline__ R muscl_left(R p1, R p2, R p3, const SchemeConst<R>& k) {
+  R Dbm, Dbp;
+  muscl_slopes(p1, p2, p3, k.limiter, Dbm, Dbp);
+  return p2 + R(0.25) * (k.omk * Dbm + k.opk * Dbp);
+}
+// wind = +1: right state of the face left of p2.
+template <class R>
+__device__ __forceinline__ R muscl_right(R p1, R p2, R p3, const SchemeConst<R>& k) {
+  R Dbm, Dbp;
+  muscl_slopes(p1, p2, p3, k.limiter, Dbm, Dbp);
+  return p2 - R(0.25) * (k.omk * Dbp + k.opk * Dbm);
+}
+
+// ------------------------------------------------------------ WENO
+// scheme_WENO.f90:87-121 (WENO_JS on u0..u4, value at the right face of u2).
+// textbook != 0: IS_1 with (u1-u3)^2 (Jiang & Shu); 0: (u1+u3)^2 as written.
+template <class R, bool EX>
+__device__ __forceinline__ R weno5(R u0, R u1, R u2, R u3, R u4, int textbook) {
+  const R q0 = R(1.0 / 3.0) * u0 - R(7.0 / 6.0) * u1 + R(11.0 / 6.0) * u2;
+  const R q1 = R(-1.0 / 6.0) * u1 + R(5.0 / 6.0) * u2 + R(1.0 / 3.0) * u3;
+  const R q2 = R(1.0 / 3.0) * u2 + R(5.0 / 6.0) * u3 - R(1.0 / 6.0) * u4;
+  const R a0 = u0 - R(2.0) * u1 + u2;
+  const R b0 = u0 - R(4.0) * u1 + R(3.0) * u2;
+  const R a1 = u1 - R(2.0) * u2 + u3;
+  const R b1 = textbook ? (u1 - u3) : (u1 + u3);
+  const R a2 = u2 - R(2.0) * u3 + u4;
+  const R b2 = R(3.0) * u2 - R(4.0) * u3 + u4;
+  const R IS0 = R(13.0 / 12.0) * (a0 * a0) + R(1.0 / 4.0) * (b0 * b0);
+  const R IS1 = R(13.0 / 12.0) * (a1 * a1) + R(1.0 / 4.0) * (b1 * b1);
+  const R IS2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
+  const R e0 = IS0 + R(1.0e-6), e1 = IS1 + R(1.0e-6), e2 = IS2 + R(1.0e-6);
+  if constexpr (EX) {
+    const R al0 = R(0.1) / (e0 * e0);
+    const R al1 = R(0.6) / (e1 * e1);
+    const R al2 = R(0.3) / (e2 * e2);
+    const R as = al0 + al1 + al2;
+    const R w0 = al0 / as, w1 = al1 / as, w2 = al2 / as;
+    return w0 * q0 + w1 * q1 + w2 * q2;
+  } else {
+    // omega_k = (c_k / d_k) / sum_j (c_j / d_j) = c_k prod_{j!=k} d_j / D
+    const R d0 = e0 * e0, d1 = e1 * e1, d2 = e2 * e2;
+    const R t0 = R(0.1) * (d1 * d2);
+    const R t1 = R(0.6) * (d0 * d2);
+    const R t2 = R(0.3) * (d0 * d1);
+    return (t0 * q0 + t1 * q1 + t2 * q2) * rcp_(t0 + t1 + t2);
+  }
+}
+
+// ------------------------------------------------------------ Roe
+// scheme_FDS_Roe.f90:25-177
+template <class R> __device__ __forceinline__ R entropy_fix_(R lam, R delta) {
+  return (lam > delta) ? lam : R(0.5) * (lam * lam + delta * delta) / delta;
+}
+
+template <int DIR, class R, bool EX>
+__device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, const SchemeConst<R>& k,
+                                         R F[5]) {
+  const R Vc_l = nrm_<DIR>(L.u, L.v, L.w);
+  const R Vc_r = nrm_<DIR>(Rs.u, Rs.v, Rs.w);
+  R H_l, H_r, rho_b, u_b, v_b, w_b, H_b;
+  if constexpr (EX) {
+    H_l = k.goverg1 * L.p / L.r + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
+    H_r = k.goverg1 * Rs.p / Rs.r + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
+    rho_b = sqrt_(L.r * Rs.r);
+    u_b = (L.r * L.u + rho_b * Rs.u) / (L.r + rho_b);
+    v_b = (L.r * L.v + rho_b * Rs.v) / (L.r + rho_b);
+    w_b = (L.r * L.w + rho_b * Rs.w) / (L.r + rho_b);
+    H_b = (L.r * H_l + rho_b * H_r) / (L.r + rho_b);
+  } else {
+    H_l = k.goverg1 * L.p * rcp_(L.r) + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
+    H_r = k.goverg1 * Rs.p * rcp_(Rs.r) + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
+    rho_b = sqrt_(L.r * Rs.r);
+    const R id = rcp_(L.r + rho_b);
+    u_b = (L.r * L.u + rho_b * Rs.u) * id;
+    v_b = (L.r * L.v + rho_b * Rs.v) * id;
+    w_b = (L.r * L.w + rho_b * Rs.w) * id;
+    H_b = (L.r * H_l + rho_b * H_r) * id;
+  }
+  const R drho = Rs.r - L.r, du = Rs.u - L.u, dv = Rs.v - L.v, dw = Rs.w - L.w;
+  const R dp = Rs.p - L.p, dVl = Vc_r - Vc_l;
+  const R Vl_b = nrm_<DIR>(u_b, v_b, w_b);
+  const R q2_b = u_b * u_b + v_b * v_b + w_b * w_b;
+  const R c_b = sqrt_(k.gm1 * (H_b - R(0.5) * q2_b));
+  const R delta = k.fix * abs_(Vl_b + c_b);
+  const R lam1 = entropy_fix_(abs_(Vl_b - c_b), delta);
+  const R lam2 = entropy_fix_(abs_(Vl_b), delta);
+  const R lam5 = entropy_fix_(abs_(Vl_b + c_b), delta);
+  R d1_0, d234_0, d5_0;
+  if constexpr (EX) {
+    d1_0 = lam1 * (dp - rho_b * c_b * dVl) / (R(2.0) * c_b * c_b);
+    d234_0 = lam2 * (drho - dp / (c_b * c_b));
+    d5_0 = lam5 * (dp + rho_b * c_b * dVl) / (R(2.0) * c_b * c_b);
+  } else {
+    const R ic2 = rcp_(c_b * c_b);
+    d1_0 = lam1 * (dp - rho_b * c_b * dVl) * (R(0.5) * ic2);
+    d234_0 = lam2 * (drho - dp * ic2);
+    d5_0 = lam5 * (dp + rho_b * c_b * dVl) * (R(0.5) * ic2);
+  }
+  const R ub[3] = {u_b, v_b, w_b};
+  const R dd[3] = {du, dv, dw};
+  const R ul[3] = {L.u, L.v, L.w};
+  const R ur[3] = {Rs.u, Rs.v, Rs.w};
+  const R l2r = lam2 * rho_b;
+  // mass
+  F[0] = R(0.5) * ((L.r * Vc_l + Rs.r * Vc_r) - (d1_0 + d234_0 + d5_0));
+  // momentum
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const R d1m = d1_0 * (m == DIR ? ub[m] - c_b : ub[m]);
+    const R d234m = d234_0 * ub[m] + l2r * (m == DIR ? dd[m] - dVl : dd[m]);
+    const R d5m = d5_0 * (m == DIR ? ub[m] + c_b : ub[m]);
+    const R flm = (m == DIR) ? L.r * ul[m] * Vc_l + L.p : L.r * ul[m] * Vc_l;
+    const R frm = (m == DIR) ? Rs.r * ur[m] * Vc_r + Rs.p : Rs.r * ur[m] * Vc_r;
+    F[1 + m] = R(0.5) * ((flm + frm) - (d1m + d234m + d5m));
+  }
+  // energy
+  {
+    const R d1e = d1_0 * (H_b - c_b * Vl_b);
+    const R d234e = d234_0 * R(0.5) * q2_b + l2r * (u_b * du + v_b * dv + w_b * dw - Vl_b * dVl);
+    const R d5e = d5_0 * (H_b + c_b * Vl_b);
+    F[4] = R(0.5) * ((L.r * H_l * Vc_l + Rs.r * H_r * Vc_r) - (d1e + d234e + d5e));
+  }
+}
+
+// ------------------------------------------------------------ Van Leer FVS
+// scheme_FVS_VanLeer.f90:25-126; textbook: supersonic sides carry the full or
+// no flux.
+template <int DIR, class R, bool EX>
+__device__ __forceinline__ void euler_flux_(const Prim5<R>& s, const SchemeConst<R>& k, R F[5]) {
+  const R Vc = nrm_<DIR>(s.u, s.v, s.w);
+  R H;
+  if constexpr (EX)
+    H = k.goverg1 * s.p / s.r + R(0.5) * (s.u * s.u + s.v * s.v + s.w * s.w);
+  else
+    H = k.goverg1 * s.p * rcp_(s.r) + R(0.5) * (s.u * s.u + s.v * s.v + s.w * s.w);
+  const R uu[3] = {s.u, s.v, s.w};
+  F[0] = s.r * Vc;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) F[1 + m] = (m == DIR) ? s.r * uu[m] * Vc + s.p : s.r * uu[m] * Vc;
+  F[4] = s.r * H * Vc;
+}
+
+template <int DIR, class R, bool EX, int SIDE /* +1 left/plus, -1 right/minus */>
+__device__ __forceinline__ void vanleer_half(const Prim5<R>& s, const SchemeConst<R>& k, R F[5]) {
+  const R Vc = nrm_<DIR>(s.u, s.v, s.w);
+  const R q2 = s.u * s.u + s.v * s.v + s.w * s.w;
+  R c, M;
+  if constexpr (EX) {
+    c = sqrt_(k.gamma * s.p / s.r);
+    M = Vc / c;
+  } else {
+    c = sqrt_(k.gamma * s.p * rcp_(s.r));
+    M = Vc * rcp_(c);
+  }
+  if (k.textbook) {
+    if ((SIDE > 0 && M >= R(1.0)) || (SIDE < 0 && M <= R(-1.0))) {
+      euler_flux_<DIR, R, EX>(s, k, F);
+      return;
+    }
+    if ((SIDE > 0 && M <= R(-1.0)) || (SIDE < 0 && M >= R(1.0))) {
+      F[0] = F[1] = F[2] = F[3] = F[4] = R(0.0);
+      return;
+    }
+  }
+  R Ms;
+  if (SIDE > 0)
+    Ms = (M >= R(1.0)) ? M : ((M <= R(-1.0)) ? R(0.0) : R(0.25) * (M + R(1.0)) * (M + R(1.0)));
+  else
+    Ms = (M >= R(1.0)) ? R(0.0) : ((M <= R(-1.0)) ? M : -(R(0.25) * (M - R(1.0)) * (M - R(1.0))));
+  const R f0 = s.r * c * Ms;
+  const R uu[3] = {s.u, s.v, s.w};
+  R tn, t;
+  if (SIDE > 0) {
+    t = k.gm1 * Vc + R(2.0) * c;
+    tn = EX ? (-Vc + R(2.0) * c) / k.gamma : (-Vc + R(2.0) * c) * rcp_(k.gamma);
+  } else {
+    t = k.gm1 * Vc - R(2.0) * c;
+    tn = EX ? (-Vc - R(2.0) * c) / k.gamma : (-Vc - R(2.0) * c) * rcp_(k.gamma);
+  }
+  F[0] = f0;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) F[1 + m] = f0 * ((m == DIR) ? tn + uu[m] : uu[m]);
+  if constexpr (EX)
+    F[4] = f0 * (t * t / k.two_g2m1 + (q2 - Vc * Vc) / R(2.0));
+  else
+    F[4] = f0 * (t * t * rcp_(k.two_g2m1) + (q2 - Vc * Vc) * R(0.5));
+}
+
+template <int DIR, class R, bool EX>
+__device__ __forceinline__ void flux_vanleer(const Prim5<R>& L, const Prim5<R>& Rs, const SchemeConst<R>& k,
+                                             R F[5]) {
+  R fp[5], fm[5];
+  vanleer_half<DIR, R, EX, +1>(L, k, fp);
+  vanleer_half<DIR, R, EX, -1>(Rs, k, fm);
+#pragma unroll
+  for (int e = 0; e < 5; ++e) F[e] = fp[e] + fm[e];
+}
+
+// ------------------------------------------------------------ AUSM
+// scheme_AUSM.f90:27-171 (beta = alpha = 0; Harten-type |M| fix, delta 0.1)
+template <int DIR, class R, bool EX>
+__device__ __forceinline__ void flux_ausm(const Prim5<R>& L, const Prim5<R>& Rs, const SchemeConst<R>& k,
+                                          R F[5]) {
+  const R Vc_l = nrm_<DIR>(L.u, L.v, L.w);
+  const R Vc_r = nrm_<DIR>(Rs.u, Rs.v, Rs.w);
+  R H_l, H_r, c_l, c_r, M_l, M_r;
+  if constexpr (EX) {
+    H_l = k.goverg1 * L.p / L.r + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
+    H_r = k.goverg1 * Rs.p / Rs.r + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
+    c_l = sqrt_(k.gamma * L.p / L.r);
+    c_r = sqrt_(k.gamma * Rs.p / Rs.r);
+    M_l = Vc_l / c_l;
+    M_r = Vc_r / c_r;
+  } else {
+    const R irl = rcp_(L.r), irr = rcp_(Rs.r);
+    H_l = k.goverg1 * L.p * irl + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
+    H_r = k.goverg1 * Rs.p * irr + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
+    c_l = sqrt_(k.gamma * L.p * irl);
+    c_r = sqrt_(k.gamma * Rs.p * irr);
+    M_l = Vc_l * rcp_(c_l);
+    M_r = Vc_r * rcp_(c_r);
+  }
+  // Mach_Split_AUSM(M_l, +1) + Mach_Split_AUSM(M_r, -1)
+  const R ms_l = (abs_(M_l) >= R(1.0)) ? R(0.5) * (M_l + abs_(M_l)) : R(0.25) * ((M_l + R(1.0)) * (M_l + R(1.0)));
+  const R ms_r = (abs_(M_r) >= R(1.0)) ? R(0.5) * (M_r - abs_(M_r))
+                                       : -(R(0.25) * ((M_r - R(1.0)) * (M_r - R(1.0))));
+  const R Mn = ms_l + ms_r;
+  const R am = abs_(Mn);
+  const R dlt = R(0.1);
+  R Mabs;
+  if constexpr (EX)
+    Mabs = (am > dlt) ? am : R(0.5) * (am * am + dlt * dlt) / dlt;
+  else
+    Mabs = (am > dlt) ? am : (am * am + dlt * dlt) * R(5.0);
+  // Pressure_Split_AUSM(p_l, M_l, +1) + Pressure_Split_AUSM(p_r, M_r, -1)
+  const R ps_l = (abs_(M_l) >= R(1.0)) ? R(0.5) * (R(1.0) + sgn1_(M_l))
+                                       : R(0.25) * ((M_l + R(1.0)) * (M_l + R(1.0))) * (R(2.0) - M_l);
+  const R ps_r = (abs_(M_r) >= R(1.0)) ? R(0.5) * (R(1.0) - sgn1_(M_r))
+                                       : R(0.25) * ((M_r - R(1.0)) * (M_r - R(1.0))) * (R(2.0) + M_r);
+  const R p_ = ps_l * L.p + ps_r * Rs.p;
+  const R wl = R(0.5) * (Mn + Mabs), wr = R(0.5) * (Mn - Mabs);
+  const R phl = L.r * c_l, phr = Rs.r * c_r;
+  F[0] = wl * phl + wr * phr;
+  F[1] = wl * (phl * L.u) + wr * (phr * Rs.u);
+  F[2] = wl * (phl * L.v) + wr * (phr * Rs.v);
+  F[3] = wl * (phl * L.w) + wr * (phr * Rs.w);
+  F[1 + DIR] = F[1 + DIR] + p_;
+  F[4] = wl * (phl * H_l) + wr * (phr * H_r);
+}
+
+template <int FLUX, int DIR, class R, bool EX>
+__device__ __forceinline__ void face_flux(const Prim5<R>& L, const Prim5<R>& Rs, const SchemeConst<R>& k,
+                                          R F[5]) {
+  if constexpr (FLUX == FLUX_ROE_)
+    flux_roe<DIR, R, EX>(L, Rs, k, F);
+  else if constexpr (FLUX == FLUX_VANLEER_)
+    flux_vanleer<DIR, R, EX>(L, Rs, k, F);
+  else
+    flux_ausm<DIR, R, EX>(L, Rs, k, F);
+}
+
+}  // namespace fvm

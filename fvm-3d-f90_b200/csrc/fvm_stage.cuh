@@ -1,0 +1,558 @@
+// fvm_stage.cuh — the fused Runge-Kutta stage kernel.
+//
+// One launch performs one RK stage over every tile of every block in a work
+// list: the per-direction loops of ClassSpaceDiscret%inviscid_flux
+// (class_space_discret.f90:120-176: reconstruct, flux, update_residual),
+// TimeScheme%Runge_Kutta (scheme_Runge_Kutta.f90:30-63) and, on the last
+// stage, the rhs^2 sums of ClassIteration%compute_residual and the wave-speed
+// maximum the next CFL time step needs.
+//
+// A task is a TX x TY column tile of one block over a z range [z0, z1).
+// The CTA marches the tile along z:
+//   * the z stencil of each column lives in a register window (planes
+//     k-1 .. k+H), refilled by one coalesced plane load per step;
+//   * plane k with its x/y halo (H cells, no corners) sits in shared memory;
+//   * each face flux is computed once and kept in shared memory (x, y) or in
+//     registers (z), and the cell's rhs is the reference's sum
+//       rhs = ((0 - dFx/dx) - dFy/dy) - dFz/dz.
+// CTAs pull tasks from an atomic counter (persistent work queue), so blocks
+// of uneven size and independent cases share one launch.
+//
+// Halo cells outside a block are read with the region rule of the block:
+// transmissive regions clamp the index to the boundary cell (the values
+// update_ghost_cell_sub, defs_block_data.f90:226-256, copies there); connected
+// and periodic regions read the ghost storage the gather kernel fills.
+#pragma once
+#include "fvm_schemes.cuh"
+#include "fvm_types.h"
+
+namespace fvm {
+
+template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY>
+struct StageCfg {
+  using R = typename PrecT<PREC>::R;
+  static constexpr bool EX = PrecT<PREC>::ex;
+  static constexpr int H = RECON == RECON_WENO_ ? 3 : (RECON == RECON_MUSCL_ ? 2 : 1);
+  static constexpr int NT = TX * TY;
+  static constexpr int PW = TX + 2 * H, PH = TY + 2 * H;
+  static constexpr int NODEV = RECON == RECON_WENO_ ? (TB ? 10 : 5) : 0;
+  static constexpr int NXN = (TX + 2) * TY, NYN = TX * (TY + 2);
+  static constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);
+  static constexpr int NW = 2 * H * (TX + TY);             // halo cells of a plane
+  static constexpr int NPL = (DIM == 2 ? NT : 0) + NW;     // plane cells loaded from HBM
+  static constexpr int NPS = (NPL + NT - 1) / NT;          // per-thread load slots
+  static constexpr int WIN = H + 2;                        // z window: planes k-1 .. k+H
+  static constexpr int WZ = RECON == RECON_WENO_ ? 2 : 1;  // warm-up planes before z0
+  static constexpr size_t smem_bytes =
+      sizeof(R) * (size_t)(5 * PH * PW + NODEV * (NXN + NYN) + 5 * (NXF + NYF));
+};
+
+// ---------------------------------------------------------------- helpers
+struct BGeo {
+  int n0, n1, n2, sy, sz, mask;
+};
+
+__device__ __forceinline__ int64_t cell_off(const BGeo& g, int x, int y, int z) {
+  x = max(x, -kGhost);
+  x = min(x, g.n0 + kGhost - 1);
+  y = max(y, -kGhost);
+  y = min(y, g.n1 + kGhost - 1);
+  z = max(z, -kGhost);
+  z = min(z, g.n2 + kGhost - 1);
+  if (x < 0 && !(g.mask & 1)) x = 0;
+  if (x >= g.n0 && !(g.mask & 2)) x = g.n0 - 1;
+  if (y < 0 && !(g.mask & 4)) y = 0;
+  if (y >= g.n1 && !(g.mask & 8)) y = g.n1 - 1;
+  if (z < 0 && !(g.mask & 16)) z = 0;
+  if (z >= g.n2 && !(g.mask & 32)) z = g.n2 - 1;
+  return (int64_t)x + (int64_t)y * g.sy + (int64_t)z * g.sz;
+}
+
+__device__ __forceinline__ void ld5(const double* __restrict__ base, int64_t off, int64_t vs, double q[5]) {
+#pragma unroll
+  for (int v = 0; v < 5; ++v) q[v] = __ldg(base + off + v * vs);
+}
+
+// Stencil value stored for reconstruction: conservative for WENO (the
+// reference reconstructs q, scheme_WENO.f90:28-72), primitive otherwise
+// (MUSCL / simple reconstruct p, scheme_reconstruct_MUSCL.f90:47-104).
+template <int RECON, class R, bool EX>
+__device__ __forceinline__ void to_stencil(const double q[5], R s[5], double gm1d, R gm1) {
+  if constexpr (RECON == RECON_WENO_) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) s[v] = (R)q[v];
+  } else {
+    if constexpr (sizeof(R) == 8) {
+      Prim5<double> p = cons2prim<double, EX>(q[0], q[1], q[2], q[3], q[4], gm1d);
+      s[0] = p.r; s[1] = p.u; s[2] = p.v; s[3] = p.w; s[4] = p.p;
+    } else {
+      Prim5<R> p = cons2prim<R, false>((R)q[0], (R)q[1], (R)q[2], (R)q[3], (R)q[4], gm1);
+      s[0] = p.r; s[1] = p.u; s[2] = p.v; s[3] = p.w; s[4] = p.p;
+    }
+  }
+}
+
+template <class R> __device__ __forceinline__ Prim5<R> mkprim(const R s[5]) {
+  Prim5<R> p;
+  p.r = s[0]; p.u = s[1]; p.v = s[2]; p.w = s[3]; p.p = s[4];
+  return p;
+}
+
+// Wave-speed sum of one cell, sum_d (|u_d| + c) / dr_d, from conservative
+// values, exact FP64 (the CFL time step of the host runtime).
+__device__ __forceinline__ double wavespeed(const double q[5], double gamma, double gm1, const double dr[3],
+                                            int idim) {
+  Prim5<double> p = cons2prim<double, true>(q[0], q[1], q[2], q[3], q[4], gm1);
+  const double c = sqrt(gamma * p.p / p.r);
+  double s = (fabs(p.u) + c) / dr[0] + (fabs(p.v) + c) / dr[1];
+  if (idim == 3) s = s + (fabs(p.w) + c) / dr[2];
+  return s;
+}
+
+// Deterministic CTA reduction of 5 sums and 1 max into partials[slot].
+template <int NT>
+__device__ __forceinline__ void cta_reduce_store(double ss[5], double wm, double* red, double* dst) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = NT / 32;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) ss[v] += __shfl_xor_sync(0xffffffffu, ss[v], o);
+    wm = fmax(wm, __shfl_xor_sync(0xffffffffu, wm, o));
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) red[v * NWARP + warp] = ss[v];
+    red[5 * NWARP + warp] = wm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[5] = {0, 0, 0, 0, 0}, m = 0.0;
+    for (int w = 0; w < NWARP; ++w) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) t[v] += red[v * NWARP + w];
+      m = fmax(m, red[5 * NWARP + w]);
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) dst[v] = t[v];
+    dst[5] = m;
+  }
+  __syncthreads();
+}
+
+// Map a plane-load index w to shared-memory plane coordinates (xx, yy).
+template <int TX, int TY, int H, int DIM>
+__device__ __forceinline__ void plane_cell(int w, int& xx, int& yy) {
+  if (DIM == 2) {
+    if (w < TX * TY) {
+      xx = H + w % TX;
+      yy = H + w / TX;
+      return;
+    }
+    w -= TX * TY;
+  }
+  if (w < 2 * H * TY) {
+    const int side = w / (H * TY), r = w % (H * TY);
+    xx = (side ? H + TX : 0) + r % H;
+    yy = H + r / H;
+  } else {
+    w -= 2 * H * TY;
+    const int side = w / (H * TX), r = w % (H * TX);
+    xx = H + r % TX;
+    yy = (side ? H + TY : 0) + r / TX;
+  }
+}
+
+// ---------------------------------------------------------------- kernel
+template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY>
+__global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
+  using C = StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>;
+  using R = typename C::R;
+  constexpr bool EX = C::EX;
+  constexpr int H = C::H, NT = C::NT, PW = C::PW, PH = C::PH;
+  constexpr int PLANE = PH * PW;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sP = reinterpret_cast<R*>(smem_raw);   // [5][PH][PW]   plane k + halo
+  R* sN = sP + 5 * PLANE;                   // [NODEV][NXN+NYN] x/y WENO nodes
+  R* sF = sN + C::NODEV * (C::NXN + C::NYN);  // [5][NXF+NYF]  x/y face fluxes
+  __shared__ double s_red[6 * (NT / 32)];
+  __shared__ int s_task;
+
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+
+  for (;;) {
+    if (tid == 0) s_task = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int ti = s_task;
+    __syncthreads();
+    if (ti >= a.ntasks) break;
+
+    const Task T = a.tasks[ti];
+    const DevBlock& B = a.blocks[T.blk];
+    const DevCase& CS = a.cases[B.case_id];
+    const double dtg = a.cstate[B.case_id].dt;
+    const double* __restrict__ qin = B.q[a.rin];
+    double* qout = B.q[a.rout];
+    const double* q0p = B.q[a.rq0];
+    double* accp = B.q[a.racc];
+    const int64_t vs = B.vs;
+    const double gm1d = CS.gm1;
+
+    SchemeConst<R> K;
+    K.gamma = (R)CS.gamma;
+    K.gm1 = (R)CS.gm1;
+    K.goverg1 = (R)(CS.gamma / CS.gm1);
+    K.two_g2m1 = (R)(2.0 * (CS.gamma * CS.gamma - 1.0));
+    K.fix = (R)CS.entropy_fix;
+    K.kappa = (R)CS.kappa;
+    K.omk = (R)(1.0 - CS.kappa);
+    K.opk = (R)(1.0 + CS.kappa);
+    K.limiter = CS.limiter;
+    K.textbook = CS.compat;
+    BGeo G;
+    G.n0 = B.n[0]; G.n1 = B.n[1]; G.n2 = B.n[2];
+    G.sy = B.sy; G.sz = B.sz; G.mask = B.ghost_mask;
+    const double dr0 = B.dr[0], dr1 = B.dr[1], dr2 = B.dr[2];
+    const double idr0 = B.inv_dr[0], idr1 = B.inv_dr[1], idr2 = B.inv_dr[2];
+    const double drv[3] = {dr0, dr1, dr2};
+    const int rk_stages = CS.rk_stages, ts_set = CS.timestep_set, idim = CS.idim;
+    const double cfl = CS.cfl, gammad = CS.gamma;
+    const double* visc = B.visc;
+    double* rhs_out = a.last ? B.rhs : nullptr;
+
+    const int nxt = min(TX, G.n0 - T.x0), nyt = min(TY, G.n1 - T.y0);
+    const bool act = tx < nxt && ty < nyt;
+    const int gx = T.x0 + tx, gy = T.y0 + ty;
+
+    double ss[5] = {0, 0, 0, 0, 0};
+    double wmax = 0.0;
+
+    // ---- z window (3D) --------------------------------------------------
+    R zw[C::WIN][5];
+    Prim5<R> zWprev;       // WENO: node value of plane k (ref: left-biased; TB: minus side)
+    R zFprev[5] = {0, 0, 0, 0, 0};
+    const int kstart = (DIM == 3) ? T.z0 - C::WZ : T.z0;
+    if constexpr (DIM == 3) {
+#pragma unroll
+      for (int s = 0; s < C::WIN; ++s) {
+        double q[5];
+        ld5(qin, cell_off(G, gx, gy, kstart - 1 + s), vs, q);
+        to_stencil<RECON, R, EX>(q, zw[s], gm1d, K.gm1);
+      }
+    } else {
+      // 2D: plane z0 into shared memory up front
+      for (int w = tid; w < C::NPL; w += NT) {
+        int xx, yy;
+        plane_cell<TX, TY, H, DIM>(w, xx, yy);
+        double q[5];
+        R s[5];
+        ld5(qin, cell_off(G, T.x0 + xx - H, T.y0 + yy - H, T.z0), vs, q);
+        to_stencil<RECON, R, EX>(q, s, gm1d, K.gm1);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) sP[v * PLANE + yy * PW + xx] = s[v];
+      }
+      __syncthreads();
+    }
+
+    for (int k = kstart; k < T.z1; ++k) {
+      const bool do_xy = (k >= T.z0);
+      const bool more = (k + 1 < T.z1);
+
+      // ---- prefetch the next plane's halo (and z window plane) into registers
+      double pre[C::NPS][5];
+      double zpre[5];
+#pragma unroll
+      for (int sidx = 0; sidx < C::NPS; ++sidx) {
+        const int w = tid + sidx * NT;
+        if (more && w < C::NPL) {
+          int xx, yy;
+          plane_cell<TX, TY, H, DIM>(w, xx, yy);
+          ld5(qin, cell_off(G, T.x0 + xx - H, T.y0 + yy - H, k + 1), vs, pre[sidx]);
+        }
+      }
+      if constexpr (DIM == 3) {
+        if (more) ld5(qin, cell_off(G, gx, gy, k + H + 1), vs, zpre);
+      }
+
+      // ---- phase A: WENO nodes --------------------------------------------
+      Prim5<R> zWcur, zWm_cur;
+      if constexpr (RECON == RECON_WENO_) {
+        if constexpr (DIM == 3) {
+          // node of plane k+1 from planes k-1 .. k+3 (window slots 0..4)
+          R wm[5], wp[5];
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            wm[v] = weno5<R, EX>(zw[0][v], zw[1][v], zw[2][v], zw[3][v], zw[4][v], K.textbook);
+            if (TB) wp[v] = weno5<R, EX>(zw[4][v], zw[3][v], zw[2][v], zw[1][v], zw[0][v], 1);
+          }
+          zWm_cur = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
+          if (TB)
+            zWcur = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
+          else
+            zWcur = zWm_cur;
+        }
+        if (do_xy) {
+          for (int w = tid; w < C::NXN + C::NYN; w += NT) {
+            R u[5][5];
+            if (w < C::NXN) {
+              const int c = w % (TX + 2) - 1, row = w / (TX + 2);
+              const int base = (H + row) * PW + (H + c - 2);
+#pragma unroll
+              for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s];
+            } else {
+              const int w2 = w - C::NXN;
+              const int col = w2 % TX, c = w2 / TX - 1;
+              const int base = (H + c - 2) * PW + (H + col);
+#pragma unroll
+              for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s * PW];
+            }
+            R wm[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) wm[v] = weno5<R, EX>(u[v][0], u[v][1], u[v][2], u[v][3], u[v][4], K.textbook);
+            Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
+            constexpr int NN = C::NXN + C::NYN;
+            sN[0 * NN + w] = pm.r;
+            sN[1 * NN + w] = pm.u;
+            sN[2 * NN + w] = pm.v;
+            sN[3 * NN + w] = pm.w;
+            sN[4 * NN + w] = pm.p;
+            if (TB) {
+              R wp[5];
+#pragma unroll
+              for (int v = 0; v < 5; ++v) wp[v] = weno5<R, EX>(u[v][4], u[v][3], u[v][2], u[v][1], u[v][0], 1);
+              Prim5<R> pp = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
+              sN[5 * NN + w] = pp.r;
+              sN[6 * NN + w] = pp.u;
+              sN[7 * NN + w] = pp.v;
+              sN[8 * NN + w] = pp.w;
+              sN[9 * NN + w] = pp.p;
+            }
+          }
+          __syncthreads();
+        }
+      }
+
+      // ---- phase B: fluxes ---------------------------------------------------
+      R zF[5] = {0, 0, 0, 0, 0};
+      if constexpr (DIM == 3) {
+        if (k >= T.z0 - 1) {
+          Prim5<R> L, Rr;
+          if constexpr (RECON == RECON_WENO_) {
+            L = zWprev;
+            Rr = zWcur;
+          } else if constexpr (RECON == RECON_MUSCL_) {
+            R l[5], r[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              l[v] = muscl_left(zw[0][v], zw[1][v], zw[2][v], K);
+              r[v] = muscl_right(zw[1][v], zw[2][v], zw[3][v], K);
+            }
+            L = mkprim(l);
+            Rr = mkprim(r);
+          } else {
+            L = mkprim(zw[1]);
+            Rr = mkprim(zw[2]);
+          }
+          face_flux<FLUX, 2, R, EX>(L, Rr, K, zF);
+        }
+      }
+      if (do_xy) {
+        constexpr int NN = C::NXN + C::NYN;
+        constexpr int NF = C::NXF + C::NYF;
+        for (int w = tid; w < NF; w += NT) {
+          R F[5];
+          if (w < C::NXF) {
+            const int f = w % (TX + 1), row = w / (TX + 1);
+            Prim5<R> L, Rr;
+            if constexpr (RECON == RECON_WENO_) {
+              const int nl = row * (TX + 2) + f, nr = nl + 1;
+              L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
+              L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
+              const int o = TB ? 5 : 0;
+              Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
+              Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
+            } else {
+              const int base = (H + row) * PW + (H + f);  // cell f (right of the face)
+              R l[5], r[5];
+#pragma unroll
+              for (int v = 0; v < 5; ++v) {
+                const R* pv = sP + v * PLANE + base;
+                if constexpr (RECON == RECON_MUSCL_) {
+                  l[v] = muscl_left(pv[-2], pv[-1], pv[0], K);
+                  r[v] = muscl_right(pv[-1], pv[0], pv[1], K);
+                } else {
+                  l[v] = pv[-1];
+                  r[v] = pv[0];
+                }
+              }
+              L = mkprim(l);
+              Rr = mkprim(r);
+            }
+            face_flux<FLUX, 0, R, EX>(L, Rr, K, F);
+          } else {
+            const int w2 = w - C::NXF;
+            const int col = w2 % TX, f = w2 / TX;
+            Prim5<R> L, Rr;
+            if constexpr (RECON == RECON_WENO_) {
+              const int nl = C::NXN + f * TX + col, nr = nl + TX;
+              L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
+              L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
+              const int o = TB ? 5 : 0;
+              Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
+              Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
+            } else {
+              const int base = (H + f) * PW + (H + col);
+              R l[5], r[5];
+#pragma unroll
+              for (int v = 0; v < 5; ++v) {
+                const R* pv = sP + v * PLANE + base;
+                if constexpr (RECON == RECON_MUSCL_) {
+                  l[v] = muscl_left(pv[-2 * PW], pv[-PW], pv[0], K);
+                  r[v] = muscl_right(pv[-PW], pv[0], pv[PW], K);
+                } else {
+                  l[v] = pv[-PW];
+                  r[v] = pv[0];
+                }
+              }
+              L = mkprim(l);
+              Rr = mkprim(r);
+            }
+            face_flux<FLUX, 1, R, EX>(L, Rr, K, F);
+          }
+#pragma unroll
+          for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
+        }
+      }
+      __syncthreads();
+
+      // ---- phase C: rhs, RK update, reductions -------------------------------
+      if (do_xy && act) {
+        constexpr int NF = C::NXF + C::NYF;
+        const int fxl = ty * (TX + 1) + tx;
+        const int fyl = C::NXF + ty * TX + tx;
+        const int64_t off = (int64_t)gx + (int64_t)gy * G.sy + (int64_t)k * G.sz;
+        double rhs[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const double fxr = (double)sF[v * NF + fxl + 1], fxL = (double)sF[v * NF + fxl];
+          const double fyr = (double)sF[v * NF + fyl + TX], fyL = (double)sF[v * NF + fyl];
+          double r;
+          if constexpr (EX) {
+            r = 0.0 - (fxr - fxL) / dr0;
+            r = r - (fyr - fyL) / dr1;
+            if constexpr (DIM == 3) r = r - ((double)zF[v] - (double)zFprev[v]) / dr2;
+          } else {
+            r = -(fxr - fxL) * idr0;
+            r = r - (fyr - fyL) * idr1;
+            if constexpr (DIM == 3) r = r - ((double)zF[v] - (double)zFprev[v]) * idr2;
+          }
+          rhs[v] = r;
+        }
+        if (visc) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) rhs[v] = rhs[v] + visc[off + v * vs];
+        }
+        // RK update (scheme_Runge_Kutta.f90:30-63; classic RK4 for 4 stages)
+        double u0[5], um[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          u0[v] = q0p[off + v * vs];
+          um[v] = __ldg(qin + off + v * vs);
+        }
+        double h = dtg;
+        if (ts_set == 2) h = cfl / wavespeed(u0, gammad, gm1d, drv, idim);
+        double out[5];
+        if (rk_stages == 3) {
+          if (a.m == 1) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) out[v] = u0[v] + h * rhs[v];
+          } else if (a.m == 2) {
+            const double c3 = 1.0 / 4.0 * h;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) out[v] = 3.0 / 4.0 * u0[v] + 1.0 / 4.0 * um[v] + c3 * rhs[v];
+          } else {
+            const double c3 = 2.0 / 3.0 * h;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) out[v] = 1.0 / 3.0 * u0[v] + 2.0 / 3.0 * um[v] + c3 * rhs[v];
+          }
+        } else {
+          if (a.m == 1) {
+            const double h2 = 0.5 * h;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              accp[off + v * vs] = rhs[v];
+              out[v] = u0[v] + h2 * rhs[v];
+            }
+          } else if (a.m == 2 || a.m == 3) {
+            const double hc = (a.m == 2) ? 0.5 * h : h;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              const double ac = accp[off + v * vs];
+              accp[off + v * vs] = ac + 2.0 * rhs[v];
+              out[v] = u0[v] + hc * rhs[v];
+            }
+          } else {
+            const double h6 = h / 6.0;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) out[v] = u0[v] + h6 * (accp[off + v * vs] + rhs[v]);
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) qout[off + v * vs] = out[v];
+        if (a.last) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) ss[v] += rhs[v] * rhs[v];
+          if (ts_set != 0) wmax = fmax(wmax, wavespeed(out, gammad, gm1d, drv, idim));
+          if (rhs_out) {
+            const int64_t nc = (int64_t)G.n0 * G.n1 * G.n2;
+            const int64_t r0 = gx + (int64_t)G.n0 * (gy + (int64_t)G.n1 * k);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) rhs_out[r0 + v * nc] = rhs[v];
+          }
+        }
+      }
+
+      // ---- carry, window shift and shared-memory refill ----------------------
+      if constexpr (DIM == 3) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) zFprev[v] = zF[v];
+        if constexpr (RECON == RECON_WENO_) zWprev = zWm_cur;
+#pragma unroll
+        for (int s = 0; s + 1 < C::WIN; ++s)
+#pragma unroll
+          for (int v = 0; v < 5; ++v) zw[s][v] = zw[s + 1][v];
+        if (more) {
+          to_stencil<RECON, R, EX>(zpre, zw[C::WIN - 1], gm1d, K.gm1);
+          // centre of plane k+1 is window slot 1 after the shift
+#pragma unroll
+          for (int v = 0; v < 5; ++v) sP[v * PLANE + (H + ty) * PW + (H + tx)] = zw[1][v];
+        }
+      }
+      if (more) {
+#pragma unroll
+        for (int sidx = 0; sidx < C::NPS; ++sidx) {
+          const int w = tid + sidx * NT;
+          if (w < C::NPL) {
+            int xx, yy;
+            plane_cell<TX, TY, H, DIM>(w, xx, yy);
+            R s[5];
+            to_stencil<RECON, R, EX>(pre[sidx], s, gm1d, K.gm1);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) sP[v * PLANE + yy * PW + xx] = s[v];
+          }
+        }
+      }
+      __syncthreads();
+    }
+
+    if (a.last) cta_reduce_store<NT>(ss, wmax, s_red, a.partials + (int64_t)T.slot * kPartStride);
+  }
+}
+
+}  // namespace fvm
