@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="global grid edge (cells)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--forms", default="fp32,fp64,exact",
+                    help="comma list of arms: fp32 (headline), fp64, exact")
     return ap.parse_args()
 
 
@@ -88,59 +90,55 @@ class Dist:
 
 # ---------------------------------------------------------------- clocks
 class Clocks:
-    """nvidia-smi sampling during the timed region (clocks + throttle reasons)."""
+    """Clock and throttle-reason sampling through NVML (read-only queries)
+    in a background thread during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
-    def __init__(self, index: str | None):
+    def __init__(self, index: int = 0):
         self.rows = []
-        self.proc = None
-        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
-        if index is not None:
-            cmd += ["-i", index]
+        self.ok = False
         try:
-            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.th = threading.Thread(target=self._read, daemon=True)
-            self.th.start()
-        except OSError:
-            self.proc = None
+            import pynvml as nv
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByIndex(index)
+            self.max_sm = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # noqa: BLE001
+            self.err = str(e)
+            return
+        self.stop_flag = False
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                try:
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                except AttributeError:
+                    rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                self.rows.append((sm, rs, pw))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.002)
 
     def stop(self) -> dict:
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"nvml unavailable: {getattr(self, 'err', '')}"]}
+        self.stop_flag = True
         self.th.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "", 1).isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "", 1).isdigit()]
-        pw = [float(r[3]) for r in self.rows if r[3].replace(".", "", 1).isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
-        load = [s for s in sm if mx and s > 0.3 * max(mx)] or sm
-        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
-                "power_w_max": max(pw) if pw else None, "samples": len(self.rows), "reasons": reasons}
-
-
-def bus_id() -> str | None:
-    try:
-        rt = ctypes.CDLL("libcudart.so.12")
-        buf = ctypes.create_string_buffer(64)
-        if rt.cudaDeviceGetPCIBusId(buf, 64, 0) == 0:
-            return buf.value.decode()
-    except OSError:
-        pass
-    return None
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({n for r in self.rows for n, bit in self.REASONS.items() if r[1] & bit})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_sm,
+                "power_w_max": max((r[2] for r in self.rows), default=None), "samples": len(self.rows),
+                "reasons": reasons, "source": "NVML, 2 ms sampling during the timed steps"}
 
 
 def peaks() -> dict:
@@ -184,7 +182,7 @@ def product(args, dist: Dist):
         s = fresh(prec, tile, z)
         s.step(args.warmup)
         dist.barrier()
-        clk = Clocks(bus_id()) if dist.rank == 0 else None
+        clk = Clocks(0) if dist.rank == 0 else None
         ms = tuning.time_step(s, args.steps)
         clocks = clk.stop() if clk else None
         ms_max = dist.max(ms)
@@ -195,16 +193,28 @@ def product(args, dist: Dist):
         return s, ms_max, clocks, prof, launches, (tile, z)
 
     out = {}
-    s32, ms32, clocks, prof32, launches, tz32 = timed(abi.PREC_FP32_FLUX)
-    s64, ms64, _, prof64, _, tz64 = timed(abi.PREC_FP64)
-    sx, msx, _, profx, _, tzx = timed(abi.PREC_FP64_EXACT)
+    forms = set(args.forms.split(","))
+    s32 = s64 = sx = None
+    if "fp32" in forms:
+        s32, ms32, clocks, prof32, launches, tz32 = timed(abi.PREC_FP32_FLUX)
+    if "fp64" in forms:
+        s64, ms64, clocks64, prof64, launches64, tz64 = timed(abi.PREC_FP64)
+    if "exact" in forms:
+        sx, msx, clocksx, profx, launchesx, tzx = timed(abi.PREC_FP64_EXACT)
+    if s32 is None:
+        # profiling runs of one FP64 arm only: report it in the headline slots
+        if s64 is not None:
+            s32, ms32, clocks, prof32, launches, tz32 = s64, ms64, clocks64, prof64, launches64, tz64
+            s64 = None
+        else:
+            s32, ms32, clocks, prof32, launches, tz32 = sx, msx, clocksx, profx, launchesx, tzx
+            sx = None
 
     def gcs(ms):
         return ncells * stages * dist.world / (ms * 1e-3) / 1e9
 
-    # L1 density difference of the FP32-flux form against FP64 after the same steps
-    l1 = float(np.mean([np.abs(s32.get_state(b)[0] - s64.get_state(b)[0]).mean() for b in range(nblk)]))
-    l1x = float(np.mean([np.abs(s64.get_state(b)[0] - sx.get_state(b)[0]).mean() for b in range(nblk)]))
+    def l1rho(a, b):
+        return float(np.mean([np.abs(a.get_state(i)[0] - b.get_state(i)[0]).mean() for i in range(nblk)]))
 
     # roofline of the dominant kernel (the fused stage): algorithmic bytes are
     # the FP64 state arrays each stage must read or write: RK4 stages touch
@@ -226,15 +236,23 @@ def product(args, dist: Dist):
     out["roofline"] = roof(prof32)
     out["clocks"] = clocks
     out["gpu_launches"] = launches * args.steps
-    out["fp64_plain"] = {"value": gcs(ms64), "ms_per_step": ms64, "roofline": roof(prof64), "tile_zchunk": tz64,
-                         "l1_density_vs_fp64_exact": l1x}
-    out["fp64_exact"] = {"value": gcs(msx), "ms_per_step": msx, "roofline": roof(profx), "tile_zchunk": tzx}
-    out["l1_density_err_vs_fp64"] = l1
+    if s64 is not None:
+        out["fp64_plain"] = {"value": gcs(ms64), "ms_per_step": ms64, "roofline": roof(prof64),
+                             "tile_zchunk": tz64}
+        # L1 density difference of the FP32-flux form against FP64 after the same steps
+        out["l1_density_err_vs_fp64"] = l1rho(s32, s64)
+    if sx is not None:
+        out["fp64_exact"] = {"value": gcs(msx), "ms_per_step": msx, "roofline": roof(profx), "tile_zchunk": tzx}
+        if s64 is not None:
+            out["fp64_plain"]["l1_density_vs_fp64_exact"] = l1rho(s64, sx)
+        else:
+            out["l1_density_err_vs_fp64"] = l1rho(s32, sx)
     out["tile_zchunk"] = tz32
     out["profile_ms"] = {k: round(sum(ms for p in prof32 for kk, ms in p if kk == k) / len(prof32), 4)
                          for k in ("stage", "gather", "finalize")}
-    sx.close()
-    s64.close()
+    for x in (sx, s64):
+        if x is not None:
+            x.close()
 
     # end to end through the C ABI with host buffers: every step uploads the
     # state from pinned host memory, advances one step (residuals come back)

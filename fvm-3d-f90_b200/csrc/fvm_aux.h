@@ -27,10 +27,13 @@ struct StageKernelInfo {
   int tx = 0, ty = 0;
 };
 
-// Tile shapes compiled for every scheme (index -> TX x TY).
-constexpr int kNumTiles = 2;
-constexpr int kTileTX[kNumTiles] = {32, 16};
-constexpr int kTileTY[kNumTiles] = {8, 16};
+// Tile shapes compiled for every scheme (index -> TX x TY, minimum resident
+// CTAs per SM the register allocation is capped for; 0 = 2 for the FP32 flux
+// form and 1 for FP64).
+constexpr int kNumTiles = 3;
+constexpr int kTileTX[kNumTiles] = {32, 16, 32};
+constexpr int kTileTY[kNumTiles] = {8, 16, 8};
+constexpr int kTileMinB[kNumTiles] = {0, 0, 2};
 
 // prec: 0 exact FP64, 1 FP64, 2 FP32 flux; dim 2|3; recon 200..202;
 // flux 300|301|303; tb: textbook WENO (mirrored right state); tile 0..kNumTiles-1.

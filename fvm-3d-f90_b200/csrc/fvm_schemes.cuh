@@ -39,6 +39,8 @@ __device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
 __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double abs_(double x) { return fabs(x); }
 __device__ __forceinline__ float abs_(float x) { return fabsf(x); }
 __device__ __forceinline__ double sgn1_(double x) { return copysign(1.0, x); }
@@ -176,7 +178,15 @@ __device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, 
   const R dp = Rs.p - L.p, dVl = Vc_r - Vc_l;
   const R Vl_b = nrm_<DIR>(u_b, v_b, w_b);
   const R q2_b = u_b * u_b + v_b * v_b + w_b * w_b;
-  const R c_b = sqrt_(k.gm1 * (H_b - R(0.5) * q2_b));
+  R c_b, ic2 = R(0);
+  if constexpr (EX) {
+    c_b = sqrt_(k.gm1 * (H_b - R(0.5) * q2_b));
+  } else {
+    const R a2 = k.gm1 * (H_b - R(0.5) * q2_b);
+    const R rs = rsqrt_(a2);
+    c_b = a2 * rs;
+    ic2 = rs * rs;
+  }
   const R delta = k.fix * abs_(Vl_b + c_b);
   const R lam1 = entropy_fix_(abs_(Vl_b - c_b), delta);
   const R lam2 = entropy_fix_(abs_(Vl_b), delta);
@@ -187,7 +197,6 @@ __device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, 
     d234_0 = lam2 * (drho - dp / (c_b * c_b));
     d5_0 = lam5 * (dp + rho_b * c_b * dVl) / (R(2.0) * c_b * c_b);
   } else {
-    const R ic2 = rcp_(c_b * c_b);
     d1_0 = lam1 * (dp - rho_b * c_b * dVl) * (R(0.5) * ic2);
     d234_0 = lam2 * (drho - dp * ic2);
     d5_0 = lam5 * (dp + rho_b * c_b * dVl) * (R(0.5) * ic2);
@@ -245,8 +254,10 @@ __device__ __forceinline__ void vanleer_half(const Prim5<R>& s, const SchemeCons
     c = sqrt_(k.gamma * s.p / s.r);
     M = Vc / c;
   } else {
-    c = sqrt_(k.gamma * s.p * rcp_(s.r));
-    M = Vc * rcp_(c);
+    const R a2 = k.gamma * s.p * rcp_(s.r);
+    const R rs = rsqrt_(a2);
+    c = a2 * rs;
+    M = Vc * rs;
   }
   if (k.textbook) {
     if ((SIDE > 0 && M >= R(1.0)) || (SIDE < 0 && M <= R(-1.0))) {
@@ -309,12 +320,15 @@ __device__ __forceinline__ void flux_ausm(const Prim5<R>& L, const Prim5<R>& Rs,
     M_r = Vc_r / c_r;
   } else {
     const R irl = rcp_(L.r), irr = rcp_(Rs.r);
-    H_l = k.goverg1 * L.p * irl + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
-    H_r = k.goverg1 * Rs.p * irr + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
-    c_l = sqrt_(k.gamma * L.p * irl);
-    c_r = sqrt_(k.gamma * Rs.p * irr);
-    M_l = Vc_l * rcp_(c_l);
-    M_r = Vc_r * rcp_(c_r);
+    const R pl = L.p * irl, pr = Rs.p * irr;
+    H_l = k.goverg1 * pl + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
+    H_r = k.goverg1 * pr + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
+    const R al = k.gamma * pl, ar = k.gamma * pr;
+    const R rsl = rsqrt_(al), rsr = rsqrt_(ar);
+    c_l = al * rsl;
+    c_r = ar * rsr;
+    M_l = Vc_l * rsl;
+    M_r = Vc_r * rsr;
   }
   // Mach_Split_AUSM(M_l, +1) + Mach_Split_AUSM(M_r, -1)
   const R ms_l = (abs_(M_l) >= R(1.0)) ? R(0.5) * (M_l + abs_(M_l)) : R(0.25) * ((M_l + R(1.0)) * (M_l + R(1.0)));

@@ -68,6 +68,27 @@ __device__ __forceinline__ int64_t cell_off(const BGeo& g, int x, int y, int z) 
   return (int64_t)x + (int64_t)y * g.sy + (int64_t)z * g.sz;
 }
 
+// The same rule split into its (x, y) part and its z part, so the loads of
+// a z-marching tile clamp x and y once per task.
+__device__ __forceinline__ int xy_off(const BGeo& g, int x, int y) {
+  x = max(x, -kGhost);
+  x = min(x, g.n0 + kGhost - 1);
+  y = max(y, -kGhost);
+  y = min(y, g.n1 + kGhost - 1);
+  if (x < 0 && !(g.mask & 1)) x = 0;
+  if (x >= g.n0 && !(g.mask & 2)) x = g.n0 - 1;
+  if (y < 0 && !(g.mask & 4)) y = 0;
+  if (y >= g.n1 && !(g.mask & 8)) y = g.n1 - 1;
+  return x + y * g.sy;
+}
+__device__ __forceinline__ int z_clamp(const BGeo& g, int z) {
+  z = max(z, -kGhost);
+  z = min(z, g.n2 + kGhost - 1);
+  if (z < 0 && !(g.mask & 16)) z = 0;
+  if (z >= g.n2 && !(g.mask & 32)) z = g.n2 - 1;
+  return z;
+}
+
 __device__ __forceinline__ void ld5(const double* __restrict__ base, int64_t off, int64_t vs, double q[5]) {
 #pragma unroll
   for (int v = 0; v < 5; ++v) q[v] = __ldg(base + off + v * vs);
@@ -164,8 +185,9 @@ __device__ __forceinline__ void plane_cell(int w, int& xx, int& yy) {
 }
 
 // ---------------------------------------------------------------- kernel
-template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY>
-__global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
+template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 2 : 1)))
+    stage_kernel(const StageArgs a) {
   using C = StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>;
   using R = typename C::R;
   constexpr bool EX = C::EX;
@@ -229,6 +251,22 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
     double ss[5] = {0, 0, 0, 0, 0};
     double wmax = 0.0;
 
+    // loop-invariant (x, y) parts of this thread's plane loads
+    int lxy[C::NPS], lsp[C::NPS];
+#pragma unroll
+    for (int sidx = 0; sidx < C::NPS; ++sidx) {
+      const int w = tid + sidx * NT;
+      lsp[sidx] = -1;
+      lxy[sidx] = 0;
+      if (w < C::NPL) {
+        int xx, yy;
+        plane_cell<TX, TY, H, DIM>(w, xx, yy);
+        lsp[sidx] = yy * PW + xx;
+        lxy[sidx] = xy_off(G, T.x0 + xx - H, T.y0 + yy - H);
+      }
+    }
+    const int cxy = xy_off(G, gx, gy);
+
     // ---- z window (3D) --------------------------------------------------
     R zw[C::WIN][5];
     Prim5<R> zWprev;       // WENO: node value of plane k (ref: left-biased; TB: minus side)
@@ -238,20 +276,21 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
 #pragma unroll
       for (int s = 0; s < C::WIN; ++s) {
         double q[5];
-        ld5(qin, cell_off(G, gx, gy, kstart - 1 + s), vs, q);
+        ld5(qin, (int64_t)cxy + (int64_t)z_clamp(G, kstart - 1 + s) * G.sz, vs, q);
         to_stencil<RECON, R, EX>(q, zw[s], gm1d, K.gm1);
       }
     } else {
       // 2D: plane z0 into shared memory up front
-      for (int w = tid; w < C::NPL; w += NT) {
-        int xx, yy;
-        plane_cell<TX, TY, H, DIM>(w, xx, yy);
-        double q[5];
-        R s[5];
-        ld5(qin, cell_off(G, T.x0 + xx - H, T.y0 + yy - H, T.z0), vs, q);
-        to_stencil<RECON, R, EX>(q, s, gm1d, K.gm1);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) sP[v * PLANE + yy * PW + xx] = s[v];
+      for (int sidx = 0; sidx < C::NPS; ++sidx) {
+        if (lsp[sidx] >= 0) {
+          double q[5];
+          R s[5];
+          ld5(qin, (int64_t)lxy[sidx] + (int64_t)T.z0 * G.sz, vs, q);
+          to_stencil<RECON, R, EX>(q, s, gm1d, K.gm1);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) sP[v * PLANE + lsp[sidx]] = s[v];
+        }
       }
       __syncthreads();
     }
@@ -259,21 +298,17 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
     for (int k = kstart; k < T.z1; ++k) {
       const bool do_xy = (k >= T.z0);
       const bool more = (k + 1 < T.z1);
+      const bool more_xy = more && (k + 1 >= T.z0);  // plane k+1 lies in [z0, z1)
 
       // ---- prefetch the next plane's halo (and z window plane) into registers
       double pre[C::NPS][5];
       double zpre[5];
 #pragma unroll
       for (int sidx = 0; sidx < C::NPS; ++sidx) {
-        const int w = tid + sidx * NT;
-        if (more && w < C::NPL) {
-          int xx, yy;
-          plane_cell<TX, TY, H, DIM>(w, xx, yy);
-          ld5(qin, cell_off(G, T.x0 + xx - H, T.y0 + yy - H, k + 1), vs, pre[sidx]);
-        }
+        if (more_xy && lsp[sidx] >= 0) ld5(qin, (int64_t)lxy[sidx] + (int64_t)(k + 1) * G.sz, vs, pre[sidx]);
       }
       if constexpr (DIM == 3) {
-        if (more) ld5(qin, cell_off(G, gx, gy, k + H + 1), vs, zpre);
+        if (more) ld5(qin, (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz, vs, zpre);
       }
 
       // ---- phase A: WENO nodes --------------------------------------------
@@ -440,6 +475,14 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
         double rhs[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
+          if constexpr (sizeof(R) == 4) {
+            // FP32 flux form: difference and scale in FP32, one conversion
+            R d = (sF[v * NF + fxl] - sF[v * NF + fxl + 1]) * (R)idr0;
+            d = d + (sF[v * NF + fyl] - sF[v * NF + fyl + TX]) * (R)idr1;
+            if constexpr (DIM == 3) d = d + (zFprev[v] - zF[v]) * (R)idr2;
+            rhs[v] = (double)d;
+            continue;
+          }
           const double fxr = (double)sF[v * NF + fxl + 1], fxL = (double)sF[v * NF + fxl];
           const double fyr = (double)sF[v * NF + fyl + TX], fyL = (double)sF[v * NF + fyl];
           double r;
@@ -527,24 +570,21 @@ __global__ void __launch_bounds__(TX* TY) stage_kernel(const StageArgs a) {
         for (int s = 0; s + 1 < C::WIN; ++s)
 #pragma unroll
           for (int v = 0; v < 5; ++v) zw[s][v] = zw[s + 1][v];
-        if (more) {
-          to_stencil<RECON, R, EX>(zpre, zw[C::WIN - 1], gm1d, K.gm1);
+        if (more) to_stencil<RECON, R, EX>(zpre, zw[C::WIN - 1], gm1d, K.gm1);
+        if (more_xy) {
           // centre of plane k+1 is window slot 1 after the shift
 #pragma unroll
           for (int v = 0; v < 5; ++v) sP[v * PLANE + (H + ty) * PW + (H + tx)] = zw[1][v];
         }
       }
-      if (more) {
+      if (more_xy) {
 #pragma unroll
         for (int sidx = 0; sidx < C::NPS; ++sidx) {
-          const int w = tid + sidx * NT;
-          if (w < C::NPL) {
-            int xx, yy;
-            plane_cell<TX, TY, H, DIM>(w, xx, yy);
+          if (lsp[sidx] >= 0) {
             R s[5];
             to_stencil<RECON, R, EX>(pre[sidx], s, gm1d, K.gm1);
 #pragma unroll
-            for (int v = 0; v < 5; ++v) sP[v * PLANE + yy * PW + xx] = s[v];
+            for (int v = 0; v < 5; ++v) sP[v * PLANE + lsp[sidx]] = s[v];
           }
         }
       }

@@ -18,10 +18,10 @@
 
 namespace fvm {
 
-template <int FLUX, bool TB, int DIM, int TX, int TY>
+template <int FLUX, bool TB, int DIM, int TX, int TY, int MINB>
 static bool fill(StageKernelInfo* out) {
   using Cfg = StageCfg<FVM_RECON, FLUX, FVM_PREC, TB, DIM, TX, TY>;
-  out->fn = reinterpret_cast<const void*>(&stage_kernel<FVM_RECON, FLUX, FVM_PREC, TB, DIM, TX, TY>);
+  out->fn = reinterpret_cast<const void*>(&stage_kernel<FVM_RECON, FLUX, FVM_PREC, TB, DIM, TX, TY, MINB>);
   out->smem = Cfg::smem_bytes;
   out->threads = TX * TY;
   out->tx = TX;
@@ -32,8 +32,9 @@ static bool fill(StageKernelInfo* out) {
 template <int FLUX, bool TB, int DIM>
 static bool by_tile(int tile, StageKernelInfo* out) {
   switch (tile) {
-    case 0: return fill<FLUX, TB, DIM, kTileTX[0], kTileTY[0]>(out);
-    case 1: return fill<FLUX, TB, DIM, kTileTX[1], kTileTY[1]>(out);
+    case 0: return fill<FLUX, TB, DIM, kTileTX[0], kTileTY[0], kTileMinB[0]>(out);
+    case 1: return fill<FLUX, TB, DIM, kTileTX[1], kTileTY[1], kTileMinB[1]>(out);
+    case 2: return fill<FLUX, TB, DIM, kTileTX[2], kTileTY[2], kTileMinB[2]>(out);
     default: return false;
   }
 }

@@ -194,7 +194,8 @@ int fvm_get_time(fvm_ctx* ctx, double* t, double* dt, int64_t* step);
 int fvm_last_error(const fvm_ctx* ctx, char* buf, size_t n);
 
 /* Autotuner hooks; no counterpart in the reference. fvm_tune_set forces the
- * tile shape (index 0: 32x8, 1: 16x16; -1 = heuristic) and z chunk length
+ * tile shape (index 0: 32x8, 1: 16x16, 2: 32x8 with registers capped for two
+ * resident CTAs per SM; -1 = heuristic) and z chunk length
  * (0 = heuristic) of the fused stage kernel for case `case_id`, keeping the
  * current state; fvm_tune_time_step runs `reps` full time steps (the state
  * advances) and returns the mean device time per step in ms. */

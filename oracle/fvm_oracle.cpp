@@ -617,11 +617,13 @@ void inviscid_dir(orc_ctx* c, Block& b, int dir) {
 }
 
 // Central second-order viscous flux (EXTENSION; the reference's
-// viscous_flux_sub, class_space_discret.f90:671-675, is empty). Face gradients:
+// viscous_flux_sub, class_space_discret.f90:671-675, is empty). The per-cell
+// contribution V = (dGx + dGy) + dGz is summed first and then added to the
+// inviscid rhs, rhs = rhs + V. Face gradients:
 // normal derivative from the two adjacent cells, tangential derivatives as
 // the mean of the two cells' central differences. tau with Stokes'
 // hypothesis; heat flux k dT/dx = mu*gamma/(Pr*(gamma-1)) d(p/rho)/dx.
-void viscous_dir(orc_ctx* c, Block& b, int dir) {
+void viscous_dir(orc_ctx* c, Block& b, int dir, std::vector<double>& V) {
   const fvm_config& cfg = c->cfg;
   const int idim = cfg.idimension;
   const int64_t nd = b.n[dir];
@@ -684,8 +686,7 @@ void viscous_dir(orc_ctx* c, Block& b, int dir) {
         y[t1] = l1;
         y[t2] = l2;
         int64_t r = b.ridx(y[0], y[1], y[2]);
-        for (int e = 0; e < 5; ++e)
-          b.rhs[r + e * rv] = b.rhs[r + e * rv] + (fv[(i + 1) * 5 + e] - fv[i * 5 + e]) / b.dr[dir];
+        for (int e = 0; e < 5; ++e) V[r + e * rv] = V[r + e * rv] + (fv[(i + 1) * 5 + e] - fv[i * 5 + e]) / b.dr[dir];
       }
     }
 }
@@ -813,8 +814,11 @@ void solve_one(orc_ctx* c) {
     for (auto& b : c->blocks)
       for (int dir = 0; dir < cfg.idimension; ++dir) inviscid_dir(c, b, dir);
     if (cfg.equation == FVM_EQ_NAVIER_STOKES)
-      for (auto& b : c->blocks)
-        for (int dir = 0; dir < cfg.idimension; ++dir) viscous_dir(c, b, dir);
+      for (auto& b : c->blocks) {
+        std::vector<double> V(b.rhs.size(), 0.0);
+        for (int dir = 0; dir < cfg.idimension; ++dir) viscous_dir(c, b, dir, V);
+        for (size_t i = 0; i < V.size(); ++i) b.rhs[i] = b.rhs[i] + V[i];
+      }
     for (auto& b : c->blocks) rk_update(c, b, m, dt);
     flow_update(c);
   }
