@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="global grid edge (cells)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tile", type=int, default=None, help="fixed tile index (skips the autotuner)")
+    ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk with --tile")
     ap.add_argument("--forms", default="fp32,fp64,exact",
                     help="comma list of arms: fp32 (headline), fp64, exact")
     return ap.parse_args()
@@ -172,6 +174,8 @@ def product(args, dist: Dist):
         return s
 
     def tune(prec):
+        if args.tile is not None:
+            return args.tile, args.zchunk
         s = fresh(prec)
         t, z, ms = tuning.autotune(s, ncells, use_cache=False, reps=2)
         s.close()

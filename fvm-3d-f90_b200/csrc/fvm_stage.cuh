@@ -23,6 +23,8 @@
 // update_ghost_cell_sub, defs_block_data.f90:226-256, copies there); connected
 // and periodic regions read the ghost storage the gather kernel fills.
 #pragma once
+#include <cuda_pipeline.h>
+
 #include "fvm_schemes.cuh"
 #include "fvm_types.h"
 
@@ -43,8 +45,10 @@ struct StageCfg {
   static constexpr int NPS = (NPL + NT - 1) / NT;          // per-thread load slots
   static constexpr int WIN = H + 2;                        // z window: planes k-1 .. k+H
   static constexpr int WZ = RECON == RECON_WENO_ ? 2 : 1;  // warm-up planes before z0
-  static constexpr size_t smem_bytes =
-      sizeof(R) * (size_t)(5 * PH * PW + NODEV * (NXN + NYN) + 5 * (NXF + NYF));
+  // R arrays first, then the FP64 staging of the cell's q0 / q_in / acc
+  static constexpr size_t r_elems = (size_t)(5 * PH * PW + NODEV * (NXN + NYN) + 5 * (NXF + NYF));
+  static constexpr size_t stage_off = (sizeof(R) * r_elems + 15) / 16 * 16;
+  static constexpr size_t smem_bytes = stage_off + sizeof(double) * 3 * 5 * NT;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -198,6 +202,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
   R* sP = reinterpret_cast<R*>(smem_raw);   // [5][PH][PW]   plane k + halo
   R* sN = sP + 5 * PLANE;                   // [NODEV][NXN+NYN] x/y WENO nodes
   R* sF = sN + C::NODEV * (C::NXN + C::NYN);  // [5][NXF+NYF]  x/y face fluxes
+  double* sQ = reinterpret_cast<double*>(smem_raw + C::stage_off);  // [3][5][NT] q0, q_in, acc
   __shared__ double s_red[6 * (NT / 32)];
   __shared__ int s_task;
 
@@ -243,6 +248,8 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
     const double cfl = CS.cfl, gammad = CS.gamma;
     const double* visc = B.visc;
     double* rhs_out = a.last ? B.rhs : nullptr;
+    const bool need_um = (rk_stages == 3 && a.m >= 2);
+    const bool need_acc = (rk_stages == 4 && a.m >= 2);
 
     const int nxt = min(TX, G.n0 - T.x0), nyt = min(TY, G.n1 - T.y0);
     const bool act = tx < nxt && ty < nyt;
@@ -309,6 +316,19 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       }
       if constexpr (DIM == 3) {
         if (more) ld5(qin, (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz, vs, zpre);
+      }
+
+      // ---- the cell's RK operands of plane k, copied asynchronously into
+      // shared memory; phase C waits for this thread's own copies only.
+      const int64_t off_k = (int64_t)gx + (int64_t)gy * G.sy + (int64_t)k * G.sz;
+      if (do_xy && act) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          __pipeline_memcpy_async(sQ + (0 * 5 + v) * NT + tid, q0p + off_k + v * vs, sizeof(double));
+          if (need_um) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NT + tid, qin + off_k + v * vs, sizeof(double));
+          if (need_acc) __pipeline_memcpy_async(sQ + (2 * 5 + v) * NT + tid, accp + off_k + v * vs, sizeof(double));
+        }
+        __pipeline_commit();
       }
 
       // ---- phase A: WENO nodes --------------------------------------------
@@ -471,7 +491,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
         constexpr int NF = C::NXF + C::NYF;
         const int fxl = ty * (TX + 1) + tx;
         const int fyl = C::NXF + ty * TX + tx;
-        const int64_t off = (int64_t)gx + (int64_t)gy * G.sy + (int64_t)k * G.sz;
+        const int64_t off = off_k;
         double rhs[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -502,11 +522,13 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
           for (int v = 0; v < 5; ++v) rhs[v] = rhs[v] + visc[off + v * vs];
         }
         // RK update (scheme_Runge_Kutta.f90:30-63; classic RK4 for 4 stages)
-        double u0[5], um[5];
+        double u0[5], um[5], ac[5];
+        __pipeline_wait_prior(0);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          u0[v] = q0p[off + v * vs];
-          um[v] = __ldg(qin + off + v * vs);
+          u0[v] = sQ[(0 * 5 + v) * NT + tid];
+          um[v] = need_um ? sQ[(1 * 5 + v) * NT + tid] : 0.0;
+          ac[v] = need_acc ? sQ[(2 * 5 + v) * NT + tid] : 0.0;
         }
         double h = dtg;
         if (ts_set == 2) h = cfl / wavespeed(u0, gammad, gm1d, drv, idim);
@@ -536,14 +558,13 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
             const double hc = (a.m == 2) ? 0.5 * h : h;
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-              const double ac = accp[off + v * vs];
-              accp[off + v * vs] = ac + 2.0 * rhs[v];
+              accp[off + v * vs] = ac[v] + 2.0 * rhs[v];
               out[v] = u0[v] + hc * rhs[v];
             }
           } else {
             const double h6 = h / 6.0;
 #pragma unroll
-            for (int v = 0; v < 5; ++v) out[v] = u0[v] + h6 * (accp[off + v * vs] + rhs[v]);
+            for (int v = 0; v < 5; ++v) out[v] = u0[v] + h6 * (ac[v] + rhs[v]);
           }
         }
 #pragma unroll
