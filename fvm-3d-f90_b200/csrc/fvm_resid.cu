@@ -1,0 +1,82 @@
+// fvm_resid.cu — residual norms of one block's rhs held in device memory.
+//
+// Restates ClassIteration%compute_residual_sub (class_iteration.f90,
+// file-local 210-248) for a caller that keeps rhs on the device:
+//   res2(e) = sum(rhs(:,:,:,e)^2) / (ni*nj*nk),  res2_t = sum_e res2(e) / neq
+//   R(e)    = sqrt(R(e)^2 + res2(e)),            R_t = sqrt(R_t^2 + res2_t)
+// so repeated calls over the blocks of a case accumulate exactly as the
+// reference does. The sum is deterministic: one CTA per k plane writes the
+// plane's five sums (fixed-order tree inside the CTA), then one CTA adds the
+// planes in k order.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fvm3d.h"
+
+namespace fvm {
+
+constexpr int kResidThreads = 256;
+
+__global__ void resid_plane_kernel(const double* __restrict__ rhs, int64_t ni, int64_t nj, int64_t nk,
+                                   double* __restrict__ plane_sums) {
+  __shared__ double red[5][kResidThreads];
+  const int64_t k = blockIdx.x;
+  const int64_t nplane = ni * nj;
+  const int64_t nc = nplane * nk;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int64_t c = threadIdx.x; c < nplane; c += kResidThreads) {
+#pragma unroll
+    for (int e = 0; e < 5; ++e) {
+      const double v = rhs[k * nplane + c + e * nc];
+      s[e] += v * v;
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 5; ++e) red[e][threadIdx.x] = s[e];
+  __syncthreads();
+  for (int w = kResidThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int e = 0; e < 5; ++e) red[e][threadIdx.x] += red[e][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int e = 0; e < 5; ++e) plane_sums[k * 5 + e] = red[e][0];
+}
+
+__global__ void resid_finalize_kernel(const double* __restrict__ plane_sums, int64_t ni, int64_t nj, int64_t nk,
+                                      double* __restrict__ res) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double res2[5] = {0, 0, 0, 0, 0}, res2_t = 0.0;
+  for (int e = 0; e < 5; ++e) {
+    for (int64_t k = 0; k < nk; ++k) res2[e] = res2[e] + plane_sums[k * 5 + e];
+    res2[e] = res2[e] / (double)(ni * nj * nk);
+    res2_t = res2_t + res2[e];
+  }
+  res2_t = res2_t / 5.0;
+  for (int e = 0; e < 5; ++e) res[e] = sqrt(res[e] * res[e] + res2[e]);
+  res[5] = sqrt(res[5] * res[5] + res2_t);
+}
+
+int residual_launch(const double* rhs, const int64_t nvert[3], double* res, double* scratch, cudaStream_t s) {
+  resid_plane_kernel<<<(unsigned)nvert[2], kResidThreads, 0, s>>>(rhs, nvert[0], nvert[1], nvert[2], scratch);
+  resid_finalize_kernel<<<1, 32, 0, s>>>(scratch, nvert[0], nvert[1], nvert[2], res);
+  return cudaGetLastError() == cudaSuccess ? FVM_OK : FVM_ERR_CUDA;
+}
+
+}  // namespace fvm
+
+extern "C" int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3], double* res_dev, void* stream) {
+  if (!rhs_dev || !nvert || !res_dev) return FVM_ERR_INVALID;
+  for (int d = 0; d < 3; ++d)
+    if (nvert[d] < 1) return FVM_ERR_INVALID;
+  if (nvert[2] > 0x7fffffff) return FVM_ERR_INVALID;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* scratch = nullptr;
+  if (cudaMalloc(&scratch, sizeof(double) * 5 * nvert[2]) != cudaSuccess) return FVM_ERR_NOMEM;
+  int rc = fvm::residual_launch(rhs_dev, nvert, res_dev, scratch, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) rc = FVM_ERR_CUDA;
+  cudaFree(scratch);
+  return rc;
+}

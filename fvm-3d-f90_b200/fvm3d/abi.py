@@ -170,6 +170,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "fvm_get_time": (ctypes.c_int, [vp, P(dbl), P(dbl), P(i64)]),
         "fvm_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "fvm_destroy": (ctypes.c_int, [vp]),
+        "fvm_residual_norms": (ctypes.c_int, [vp, P(i64), vp, vp]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)

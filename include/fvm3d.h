@@ -209,6 +209,17 @@ int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step);
 int fvm_profile_step(fvm_ctx* ctx, float* ms, int32_t* kinds, int cap, int* n);
 int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n);
 
+/* Residual norms of one block's rhs in device memory, as
+ * ClassIteration%compute_residual_sub (class_iteration.f90, file-local
+ * 210-248): rhs_dev is the Fortran (ni,nj,nk,5) array nvert describes;
+ * res_dev points at 6 device doubles (per equation, then R_total) that are
+ * updated as R = sqrt(R^2 + res2), so calls over the blocks of a case
+ * accumulate like the reference (zero them before the first block). Runs on
+ * `stream` (a cudaStream_t, NULL for the default stream) and returns after
+ * it completes; allocates a scratch buffer of 40 bytes per k plane for the
+ * call. */
+int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3], double* res_dev, void* stream);
+
 /* Release the context and its device memory. */
 int fvm_destroy(fvm_ctx* ctx);
 
