@@ -47,10 +47,13 @@ void Engine::release() {
   if (graph_) cudaGraphDestroy(graph_);
   gexec_ = nullptr;
   graph_ = nullptr;
-  for (auto& r : role_) {
-    if (r) cudaFree(r);
-    r = nullptr;
+  // roles beyond nroles_ alias role A: free each allocation once
+  for (int r = 0; r < NROLE; ++r) {
+    bool alias = false;
+    for (int q = 0; q < r; ++q) alias |= (role_[q] == role_[r]);
+    if (role_[r] && !alias) cudaFree(role_[r]);
   }
+  for (auto& r : role_) r = nullptr;
   void* ptrs[] = {visc_, rhs_all_, d_blocks_, d_cases_, d_state_, d_tasks_, d_partials_, d_pairs_, d_counters_,
                   d_casemax_, d_staging_};
   for (void* p : ptrs)

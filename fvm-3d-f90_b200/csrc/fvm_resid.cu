@@ -60,6 +60,7 @@ __global__ void resid_finalize_kernel(const double* __restrict__ plane_sums, int
 }
 
 int residual_launch(const double* rhs, const int64_t nvert[3], double* res, double* scratch, cudaStream_t s) {
+  (void)cudaGetLastError();  // report only the errors of these launches
   resid_plane_kernel<<<(unsigned)nvert[2], kResidThreads, 0, s>>>(rhs, nvert[0], nvert[1], nvert[2], scratch);
   resid_finalize_kernel<<<1, 32, 0, s>>>(scratch, nvert[0], nvert[1], nvert[2], res);
   return cudaGetLastError() == cudaSuccess ? FVM_OK : FVM_ERR_CUDA;
