@@ -847,6 +847,9 @@ struct fvm_ctx {
 
 static std::string g_create_error;
 
+// Message for fvm_last_error(NULL, ...) from entry points without a context.
+void fvm_internal_set_global_error(const char* msg) { g_create_error = msg ? msg : ""; }
+
 extern "C" {
 
 int fvm_abi_version(void) { return FVM3D_ABI_VERSION; }

@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/fvm3d.h"
 
 namespace fvm {
@@ -79,5 +81,73 @@ extern "C" int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3],
   int rc = fvm::residual_launch(rhs_dev, nvert, res_dev, scratch, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) rc = FVM_ERR_CUDA;
   cudaFree(scratch);
+  return rc;
+}
+
+// ---------------------------------------------------------------- no allocation
+// fvm_residual_norms_noalloc: the same two kernels, with the per-plane sums in
+// a fixed array that is part of the library image, for callers that may not
+// allocate device memory themselves (their device memory belongs to an
+// allocator they do not control: a host code that reserves the whole GPU
+// budget for its own pool at start-up, or a runtime that forbids new
+// allocations once a simulation runs). The array holds one 5-double partial
+// per k plane, so blocks up to kNoAllocMaxPlanes planes fit; every GPU that
+// loads the library keeps these 160 KiB until the process exits.
+namespace {
+
+constexpr int64_t kNoAllocMaxPlanes = 4096;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_plane_sums[kNoAllocMaxPlanes * 5];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+void fvm_internal_set_global_error(const char* msg);
+
+extern "C" int fvm_residual_norms_noalloc(const double* rhs_dev, const int64_t nvert[3], double* res_dev,
+                                          void* stream) {
+  if (!rhs_dev || !nvert || !res_dev) {
+    fvm_internal_set_global_error("fvm_residual_norms_noalloc: null argument");
+    return FVM_ERR_INVALID;
+  }
+  for (int d = 0; d < 3; ++d)
+    if (nvert[d] < 1) {
+      fvm_internal_set_global_error("fvm_residual_norms_noalloc: nvert must be >= 1");
+      return FVM_ERR_INVALID;
+    }
+  if (nvert[2] > kNoAllocMaxPlanes) {
+    fvm_internal_set_global_error(
+        "fvm_residual_norms_noalloc: nvert[2] exceeds 4096, the planes its fixed scratch array holds; "
+        "use fvm_residual_norms");
+    return FVM_ERR_INVALID;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return FVM_ERR_CUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    fvm_internal_set_global_error("fvm_residual_norms_noalloc: device ordinal above 63");
+    return FVM_ERR_UNSUPPORTED;
+  }
+  double* scratch = nullptr;
+  {
+    // once per device, with that device current: the array's device address
+    // (its name in host code is only a host-side stand-in)
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_plane_sums);
+      if (e != cudaSuccess || !p) {
+        fvm_internal_set_global_error("fvm_residual_norms_noalloc: cudaGetSymbolAddress failed");
+        return FVM_ERR_CUDA;
+      }
+      g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = fvm::residual_launch(rhs_dev, nvert, res_dev, scratch, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) rc = FVM_ERR_CUDA;
   return rc;
 }

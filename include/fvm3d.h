@@ -220,6 +220,22 @@ int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n);
  * call. */
 int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3], double* res_dev, void* stream);
 
+/* fvm_residual_norms for callers that cannot allocate device memory; no
+ * counterpart in the reference. Some host codes own every byte of GPU memory
+ * through their own pool and forbid a library from allocating: this entry
+ * point computes exactly what fvm_residual_norms computes but takes its
+ * per-plane scratch from a fixed array inside the library (160 KiB per GPU
+ * that loads it, kept until the process exits) and calls no allocator.
+ * Limit: nvert[2] <= 4096 planes; larger blocks are rejected with
+ * FVM_ERR_INVALID and a message for fvm_last_error(NULL, ...). The first
+ * call on a device looks up the array's device address (with that device
+ * current); make that first call before any stream capture. All calls share
+ * the array: calls that overlap on the GPU (other host threads, other
+ * streams) race, while calls in sequence are safe because every partial the
+ * finalize reads is written by the same call first. Returns after `stream`
+ * completes. */
+int fvm_residual_norms_noalloc(const double* rhs_dev, const int64_t nvert[3], double* res_dev, void* stream);
+
 /* Release the context and its device memory. */
 int fvm_destroy(fvm_ctx* ctx);
 
