@@ -110,15 +110,18 @@ __global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const uns
 // ClassIteration%reset_residual / compute_residual per block in block order /
 // update (class_iteration.f90, file-local 195-259), time += dt, the stop
 // checks of converged (:180-188) and the next step's dt.
-__global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, DevCaseState* st,
+__global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                                 const double* partials, int* counters, int ncounters) {
   __shared__ double red[6][256];
   const int c = blockIdx.x, tid = threadIdx.x;
   const DevCase& C = cases[c];
+  if (c == 0)
+    for (int i = tid; i < ncounters; i += blockDim.x) counters[i] = 0;
+  if (C.nblocks == 0) return;  // removed case
   double res[6] = {0, 0, 0, 0, 0, 0};
   double wmax = 0.0;
-  for (int b = C.block0; b < C.block0 + C.nblocks; ++b) {
-    const DevBlock& B = blocks[b];
+  for (int bb = 0; bb < C.nblocks; ++bb) {
+    const DevBlock& B = blocks[case_blk[C.block0 + bb]];
     double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
     for (int t = tid; t < B.ntask; t += blockDim.x) {
       const double* p = partials + (int64_t)(B.task0 + t) * kPartStride;
@@ -167,8 +170,6 @@ __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, De
       S.status = 5;  // FVM_ERR_DIVERGED
     S.dt = (C.timestep_set == 0) ? C.dt_fixed : C.cfl / wmax;
   }
-  if (c == 0)
-    for (int i = tid; i < ncounters; i += blockDim.x) counters[i] = 0;
 }
 
 // ---------------------------------------------------------------- viscous
@@ -304,9 +305,9 @@ cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* c
   return cudaGetLastError();
 }
 
-cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, DevCaseState* st, int ncases,
-                            const double* partials, int* counters, int ncounters, cudaStream_t s) {
-  finalize_kernel<<<ncases, 256, 0, s>>>(blocks, cases, st, partials, counters, ncounters);
+cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
+                            int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s) {
+  finalize_kernel<<<ncases, 256, 0, s>>>(blocks, cases, case_blk, st, partials, counters, ncounters);
   return cudaGetLastError();
 }
 

@@ -39,6 +39,8 @@ Engine::Engine() {}
 
 Engine::~Engine() {
   release();
+  for (auto s : side_) cudaStreamDestroy(s);
+  for (auto e : fork_ev_) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -54,21 +56,32 @@ void Engine::release() {
     if (role_[r] && !alias) cudaFree(role_[r]);
   }
   for (auto& r : role_) r = nullptr;
-  void* ptrs[] = {visc_, rhs_all_, d_blocks_, d_cases_, d_state_, d_tasks_, d_partials_, d_pairs_, d_counters_,
-                  d_casemax_, d_staging_};
+  void* ptrs[] = {visc_,     d_blocks_,   d_cases_,     d_case_blk_, d_state_, d_tasks_,
+                  d_partials_, d_pairs_, d_counters_, d_casemax_,  d_staging_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  visc_ = rhs_all_ = nullptr;
+  visc_ = nullptr;
   d_blocks_ = nullptr;
   d_cases_ = nullptr;
+  d_case_blk_ = nullptr;
   d_state_ = nullptr;
+  state_cap_ = 0;
   d_tasks_ = nullptr;
   d_partials_ = nullptr;
   d_pairs_ = nullptr;
   d_counters_ = nullptr;
   d_casemax_ = nullptr;
   d_staging_ = nullptr;
-  for (auto& b : blocks) b.rhs_dev = nullptr;
+  staging_bytes_ = 0;
+  for (auto& b : blocks) {
+    if (b.rhs_dev) cudaFree(b.rhs_dev);
+    b.rhs_dev = nullptr;
+    b.slab_off = -1;
+    b.fresh = true;
+  }
+  for (auto& c : cases) c.fresh = true;
+  cap_ = 0;
+  free_.clear();
   planned_ = false;
   prepared_ = false;
 }
@@ -77,14 +90,21 @@ int Engine::cuda_fail(cudaError_t e, const char* where) {
   return fail(FVM_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 
-#define CK(call)                                             \
-  do {                                                       \
-    cudaError_t e_ = (call);                                 \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call);      \
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
 
+int64_t padded_cells(int idimension, const int64_t n[3]) {
+  const int64_t px = round_up(n[0] + kPadX + kGhost, 4);
+  const int64_t py = n[1] + 2 * kGhost;
+  const int64_t pz = n[2] + 2 * (idimension == 3 ? kGhost : 0);
+  return round_up(px * py * pz, 64);
+}
+
 // ---------------------------------------------------------------- topology
-int Engine::add_case(const fvm_config& c) {
+int Engine::add_case(const fvm_config& c, int* case_id) {
   if (c.struct_size != (int32_t)sizeof(fvm_config)) return fail(FVM_ERR_INVALID, "fvm_config.struct_size mismatch");
   if (c.idimension != 2 && c.idimension != 3) return fail(FVM_ERR_INVALID, "idimension must be 2 or 3");
   if (c.equation != FVM_EQ_EULER && c.equation != FVM_EQ_NAVIER_STOKES)
@@ -114,22 +134,52 @@ int Engine::add_case(const fvm_config& c) {
   if (!(c.gamma > 1.0)) return fail(FVM_ERR_INVALID, "gamma must exceed 1");
   if (c.equation == FVM_EQ_NAVIER_STOKES && (!(c.mu >= 0.0) || !(c.prandtl > 0.0)))
     return fail(FVM_ERR_INVALID, "Navier-Stokes needs mu >= 0 and prandtl > 0");
-  if (!cases.empty() && cases[0].cfg.rk_stages != c.rk_stages)
-    return fail(FVM_ERR_INVALID, "all cases of one engine share the RK stage count");
+  for (const auto& o : cases)
+    if (!o.dead && o.cfg.rk_stages != c.rk_stages)
+      return fail(FVM_ERR_INVALID, "all cases of one engine share the RK stage count");
+  if (cap_ > 0 && nroles_ < (c.rk_stages == 4 ? 4 : 3))
+    return fail(FVM_ERR_INVALID, "the arena was laid out for 3 RK stages");
   HCase hc;
   hc.cfg = c;
   cases.push_back(hc);
-  release();
+  if (case_id) *case_id = (int)cases.size() - 1;
+  invalidate();
+  return FVM_OK;
+}
+
+int Engine::remove_case(int case_id) {
+  if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
+  HCase& hc = cases[case_id];
+  for (int b : hc.blocks) {
+    HBlock& B = blocks[b];
+    if (B.slab_off >= 0) free_range(B.slab_off, B.padded);
+    if (B.rhs_dev) cudaFree(B.rhs_dev);
+    B.rhs_dev = nullptr;
+    B.slab_off = -1;
+    B.dead = true;
+    B.conns.clear();
+  }
+  hc.dead = true;
+  invalidate();
+  return FVM_OK;
+}
+
+int Engine::reserve(int64_t cells) {
+  if (cells < 0) return fail(FVM_ERR_INVALID, "negative reservation");
+  if (cap_ > 0) return fail(FVM_ERR_STATE, "the arena is already laid out");
+  reserved_ = cells;
   return FVM_OK;
 }
 
 int Engine::add_block(int case_id, const int64_t n[3], const double dr[3], int* blk) {
-  if (case_id < 0 || case_id >= (int)cases.size()) return fail(FVM_ERR_INVALID, "bad case id");
+  if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
   if (!n || !dr) return fail(FVM_ERR_INVALID, "null nvert / dr");
   for (int d = 0; d < 3; ++d) {
     if (n[d] < 1 || n[d] > (1 << 20)) return fail(FVM_ERR_INVALID, "nvert out of range [1, 2^20]");
     if (!(dr[d] > 0.0) || !std::isfinite(dr[d])) return fail(FVM_ERR_INVALID, "dr must be positive");
   }
+  if (padded_cells(cases[case_id].cfg.idimension, n) >= ((int64_t)1 << 31))
+    return fail(FVM_ERR_INVALID, "block too large (2^31 padded cells)");
   HBlock b;
   b.case_id = case_id;
   for (int d = 0; d < 3; ++d) {
@@ -139,12 +189,12 @@ int Engine::add_block(int case_id, const int64_t n[3], const double dr[3], int* 
   blocks.push_back(b);
   cases[case_id].blocks.push_back((int)blocks.size() - 1);
   if (blk) *blk = (int)blocks.size() - 1;
-  release();
+  invalidate();
   return FVM_OK;
 }
 
 int Engine::set_boundary(int blk, int region, int kind) {
-  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (region < 1 || region > 6) return fail(FVM_ERR_INVALID, "region must be 1..6");
   HBlock& b = blocks[blk];
   const int ax = (region - 1) / 2;
@@ -186,14 +236,13 @@ int Engine::set_boundary(int blk, int region, int kind) {
     c.donor = blk;
     b.conns.push_back(c);
   }
-  release();
+  invalidate();
   return FVM_OK;
 }
 
 int Engine::connect(int blk, const int64_t range[3][2], int donor, const int64_t drange[3][2],
                     const int32_t dtype[3]) {
-  if (blk < 0 || blk >= (int)blocks.size() || donor < 0 || donor >= (int)blocks.size())
-    return fail(FVM_ERR_INVALID, "bad block id");
+  if (!live_block(blk) || !live_block(donor)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!range || !drange || !dtype) return fail(FVM_ERR_INVALID, "null range");
   int seen = 0;
   for (int a = 0; a < 3; ++a) {
@@ -251,38 +300,7 @@ int Engine::connect(int blk, const int64_t range[3][2], int donor, const int64_t
   }
   b.bc[region - 1] = FVM_BC_CONNECTED;
   b.conns.push_back(c);
-  release();
-  return FVM_OK;
-}
-
-int Engine::set_tuning(int case_id, int tile, int zchunk) {
-  if (case_id < 0 || case_id >= (int)cases.size()) return fail(FVM_ERR_INVALID, "bad case id");
-  if (tile < -1 || tile >= kNumTiles) return fail(FVM_ERR_INVALID, "bad tile index");
-  if (zchunk < 0) return fail(FVM_ERR_INVALID, "bad z chunk");
-  if (cases[case_id].tile == tile && cases[case_id].zchunk == zchunk) return FVM_OK;
-  cases[case_id].tile = tile;
-  cases[case_id].zchunk = zchunk;
-  if (!planned_) {
-    release();
-    return FVM_OK;
-  }
-  // re-plan keeping the state, time and residual history
-  std::vector<std::vector<double>> saved(blocks.size());
-  for (size_t b = 0; b < blocks.size(); ++b) {
-    saved[b].resize(5 * blocks[b].n[0] * blocks[b].n[1] * blocks[b].n[2]);
-    int rc = get_state((int)b, saved[b].data(), 0);
-    if (rc) return rc;
-  }
-  std::vector<DevCaseState> st(cases.size());
-  CK(cudaMemcpyAsync(st.data(), d_state_, sizeof(DevCaseState) * cases.size(), cudaMemcpyDeviceToHost, stream));
-  CK(cudaStreamSynchronize(stream));
-  int rc = plan();
-  if (rc) return rc;
-  CK(cudaMemcpyAsync(d_state_, st.data(), sizeof(DevCaseState) * cases.size(), cudaMemcpyHostToDevice, stream));
-  for (size_t b = 0; b < blocks.size(); ++b) {
-    rc = set_state((int)b, saved[b].data());
-    if (rc) return rc;
-  }
+  invalidate();
   return FVM_OK;
 }
 
@@ -331,30 +349,114 @@ int Engine::resolve(int blk, int64_t x[3], int* out_blk) const {
 }
 
 // ---------------------------------------------------------------- planning
+int Engine::set_tuning(int case_id, int tile, int zchunk) {
+  if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
+  if (tile < -1 || tile >= kNumTiles) return fail(FVM_ERR_INVALID, "bad tile index");
+  if (zchunk < 0) return fail(FVM_ERR_INVALID, "bad z chunk");
+  if (cases[case_id].tile == tile && cases[case_id].zchunk == zchunk) return FVM_OK;
+  cases[case_id].tile = tile;
+  cases[case_id].zchunk = zchunk;
+  invalidate();  // the arena and every case's state stay where they are
+  return FVM_OK;
+}
+
+// ---------------------------------------------------------------- arena
+int Engine::alloc_range(int64_t size, int64_t* off) {
+  for (size_t i = 0; i < free_.size(); ++i) {
+    if (free_[i].second >= size) {
+      *off = free_[i].first;
+      free_[i].first += size;
+      free_[i].second -= size;
+      if (free_[i].second == 0) free_.erase(free_.begin() + i);
+      return 0;
+    }
+  }
+  return -1;
+}
+
+void Engine::free_range(int64_t off, int64_t size) {
+  free_.push_back({off, size});
+  std::sort(free_.begin(), free_.end());
+  std::vector<std::pair<int64_t, int64_t>> m;
+  for (auto& r : free_) {
+    if (!m.empty() && m.back().first + m.back().second == r.first)
+      m.back().second += r.second;
+    else
+      m.push_back(r);
+  }
+  free_ = m;
+}
+
+// Replace the arena by one of at least `need` elements per slab, moving the
+// live blocks' boxes (all roles and the viscous slab) to their new offsets.
+int Engine::grow_arena(int64_t need) {
+  const int64_t ncap = round_up(std::max(need, cap_), 64);
+  double* nr[NROLE] = {nullptr, nullptr, nullptr, nullptr};
+  for (int r = 0; r < nroles_; ++r) {
+    cudaError_t e = cudaMalloc(&nr[r], sizeof(double) * 5 * ncap);
+    if (e != cudaSuccess) {
+      for (int q = 0; q < r; ++q) cudaFree(nr[q]);
+      return fail(FVM_ERR_NOMEM, std::string("state allocation: ") + cudaGetErrorString(e));
+    }
+    CK(cudaMemsetAsync(nr[r], 0, sizeof(double) * 5 * ncap, stream));
+  }
+  double* nv = nullptr;
+  if (visc_) {
+    CK(cudaMalloc(&nv, sizeof(double) * 5 * ncap));
+    CK(cudaMemsetAsync(nv, 0, sizeof(double) * 5 * ncap, stream));
+  }
+  // lay the live, already placed blocks out contiguously in the new arena
+  int64_t off = 0;
+  for (auto& b : blocks) {
+    if (b.dead || b.slab_off < 0) continue;
+    for (int r = 0; r < nroles_; ++r)
+      for (int v = 0; v < 5; ++v)
+        CK(cudaMemcpyAsync(nr[r] + off + v * ncap, role_[r] + b.slab_off + v * cap_, sizeof(double) * b.padded,
+                           cudaMemcpyDeviceToDevice, stream));
+    b.slab_off = off;
+    off += b.padded;
+  }
+  CK(cudaStreamSynchronize(stream));
+  for (int r = 0; r < nroles_; ++r)
+    if (role_[r]) cudaFree(role_[r]);
+  if (visc_) cudaFree(visc_);
+  for (int r = 0; r < NROLE; ++r) role_[r] = (r < nroles_) ? nr[r] : nr[ROLE_A];
+  visc_ = nv;
+  cap_ = ncap;
+  free_.clear();
+  if (off < cap_) free_.push_back({off, cap_ - off});
+  return FVM_OK;
+}
+
+// ---------------------------------------------------------------- planning
 int Engine::ensure_planned() {
   if (planned_) return FVM_OK;
   return plan();
 }
 
 int Engine::plan() {
-  release();
-  if (cases.empty()) return fail(FVM_ERR_STATE, "no case configured");
-  if (blocks.empty()) return fail(FVM_ERR_STATE, "no block added");
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  gexec_ = nullptr;
+  graph_ = nullptr;
+  std::vector<int> live_cases, live_blocks;
+  for (size_t c = 0; c < cases.size(); ++c)
+    if (!cases[c].dead) live_cases.push_back((int)c);
+  for (size_t b = 0; b < blocks.size(); ++b)
+    if (!blocks[b].dead) live_blocks.push_back((int)b);
+  if (live_cases.empty()) return fail(FVM_ERR_STATE, "no case configured");
+  if (live_blocks.empty()) return fail(FVM_ERR_STATE, "no block added");
   if (!stream) {
     CK(cudaGetDevice(&device));
     CK(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   }
-  max_stages_ = cases[0].cfg.rk_stages;
-  nroles_ = (max_stages_ == 4) ? 4 : 3;
-  bool any_ns = false, any_rhs = false;
-  for (auto& c : cases) {
-    any_ns |= c.cfg.equation == FVM_EQ_NAVIER_STOKES;
-    any_rhs |= c.cfg.store_rhs != 0;
-  }
+  max_stages_ = cases[live_cases[0]].cfg.rk_stages;
+  bool any_ns = false;
+  for (int c : live_cases) any_ns |= cases[c].cfg.equation == FVM_EQ_NAVIER_STOKES;
 
   // -- coverage of connected regions
-  for (size_t bi = 0; bi < blocks.size(); ++bi) {
+  for (int bi : live_blocks) {
     const HBlock& b = blocks[bi];
     for (int region = 1; region <= 6; ++region) {
       if (b.bc[region - 1] == FVM_BC_TRANSMISSIVE) continue;
@@ -375,17 +477,18 @@ int Engine::plan() {
       for (char v : cov)
         if (!v) {
           char m[160];
-          std::snprintf(m, sizeof m, "region %d of block %zu is connected but not every ghost cell has a donor",
+          std::snprintf(m, sizeof m, "region %d of block %d is connected but not every ghost cell has a donor",
                         region, bi);
           return fail(FVM_ERR_INVALID, m);
         }
     }
   }
 
-  // -- layout
-  int64_t off = 0;
+  // -- layout of every live block
+  int64_t need = 0;
   size_t max_cells = 0;
-  for (auto& b : blocks) {
+  for (int bi : live_blocks) {
+    HBlock& b = blocks[bi];
     const int idim = cases[b.case_id].cfg.idimension;
     b.px = round_up(b.n[0] + kPadX + kGhost, 4);
     b.py = b.n[1] + 2 * kGhost;
@@ -394,43 +497,71 @@ int Engine::plan() {
     b.sy = b.px;
     b.sz = b.px * b.py;
     b.org = kPadX + kGhost * b.sy + b.zpad * b.sz;
-    b.slab_off = off;
-    off = round_up(off + b.px * b.py * b.pz, 64);
+    b.padded = padded_cells(idim, b.n);
+    need += b.padded;
     max_cells = std::max(max_cells, (size_t)(b.n[0] * b.n[1] * b.n[2]));
   }
-  cap_ = round_up(off, 64);
-  if (cap_ >= ((int64_t)1 << 40)) return fail(FVM_ERR_INVALID, "grid too large");
-  for (int r = 0; r < nroles_; ++r) {
-    cudaError_t e = cudaMalloc(&role_[r], sizeof(double) * 5 * cap_);
-    if (e != cudaSuccess) return fail(FVM_ERR_NOMEM, std::string("state allocation: ") + cudaGetErrorString(e));
-    CK(cudaMemsetAsync(role_[r], 0, sizeof(double) * 5 * cap_, stream));
+
+  // -- the arena: created once (reserved size or exactly what is needed),
+  //    grown only in the unreserved mode
+  if (cap_ == 0) {
+    nroles_ = (max_stages_ == 4) ? 4 : 3;
+    const int64_t cap = round_up(std::max(reserved_, need), 64);
+    if (cap >= ((int64_t)1 << 40)) return fail(FVM_ERR_INVALID, "grid too large");
+    for (int r = 0; r < nroles_; ++r) {
+      cudaError_t e = cudaMalloc(&role_[r], sizeof(double) * 5 * cap);
+      if (e != cudaSuccess) return fail(FVM_ERR_NOMEM, std::string("state allocation: ") + cudaGetErrorString(e));
+      CK(cudaMemsetAsync(role_[r], 0, sizeof(double) * 5 * cap, stream));
+    }
+    for (int r = nroles_; r < NROLE; ++r) role_[r] = role_[ROLE_A];
+    cap_ = cap;
+    free_.clear();
+    free_.push_back({0, cap_});
   }
-  for (int r = nroles_; r < NROLE; ++r) role_[r] = role_[ROLE_A];
-  if (any_ns) {
+  if (any_ns && !visc_) {
     CK(cudaMalloc(&visc_, sizeof(double) * 5 * cap_));
     CK(cudaMemsetAsync(visc_, 0, sizeof(double) * 5 * cap_, stream));
   }
-  if (any_rhs) {
-    int64_t tot = 0;
-    for (auto& b : blocks)
-      if (cases[b.case_id].cfg.store_rhs) tot += 5 * b.n[0] * b.n[1] * b.n[2];
-    CK(cudaMalloc(&rhs_all_, sizeof(double) * tot));
-    CK(cudaMemsetAsync(rhs_all_, 0, sizeof(double) * tot, stream));
-    int64_t o = 0;
-    for (auto& b : blocks)
-      if (cases[b.case_id].cfg.store_rhs) {
-        b.rhs_dev = rhs_all_ + o;
-        o += 5 * b.n[0] * b.n[1] * b.n[2];
-      }
+  for (int bi : live_blocks) {
+    HBlock& b = blocks[bi];
+    if (b.slab_off >= 0) continue;
+    int64_t off = -1;
+    if (alloc_range(b.padded, &off) != 0) {
+      if (reserved_ > 0) return fail(FVM_ERR_NOMEM, "HBM budget exhausted: the reserved arena has no room");
+      int rc = grow_arena(need);
+      if (rc) return rc;
+      if (alloc_range(b.padded, &off) != 0) return fail(FVM_ERR_NOMEM, "arena allocation failed");
+    }
+    b.slab_off = off;
   }
-  staging_bytes_ = sizeof(double) * 5 * max_cells;
-  CK(cudaMalloc(&d_staging_, staging_bytes_));
+  for (int bi : live_blocks) {
+    HBlock& b = blocks[bi];
+    if (!b.fresh) continue;
+    for (int r = 0; r < nroles_; ++r)
+      for (int v = 0; v < 5; ++v)
+        CK(cudaMemsetAsync(role_[r] + b.slab_off + v * cap_, 0, sizeof(double) * b.padded, stream));
+    if (visc_)
+      for (int v = 0; v < 5; ++v)
+        CK(cudaMemsetAsync(visc_ + b.slab_off + v * cap_, 0, sizeof(double) * b.padded, stream));
+    if (cases[b.case_id].cfg.store_rhs && !b.rhs_dev) {
+      const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
+      CK(cudaMalloc(&b.rhs_dev, bytes));
+      CK(cudaMemsetAsync(b.rhs_dev, 0, bytes, stream));
+    }
+    b.fresh = false;
+  }
+  if (sizeof(double) * 5 * max_cells > staging_bytes_) {
+    if (d_staging_) cudaFree(d_staging_);
+    d_staging_ = nullptr;
+    staging_bytes_ = sizeof(double) * 5 * max_cells;
+    CK(cudaMalloc(&d_staging_, staging_bytes_));
+  }
 
   // -- groups (one per distinct kernel) and tasks
   groups.clear();
   std::vector<Task> tasks;
-  std::vector<int> block_task0(blocks.size()), block_ntask(blocks.size());
-  for (size_t ci = 0; ci < cases.size(); ++ci) {
+  std::vector<int> block_task0(blocks.size(), 0), block_ntask(blocks.size(), 0);
+  for (int ci : live_cases) {
     HCase& hc = cases[ci];
     const fvm_config& c = hc.cfg;
     const int dim = c.idimension;
@@ -438,10 +569,11 @@ int Engine::plan() {
     const bool tb = c.reconstruct == FVM_RECON_WENO && c.compat == FVM_COMPAT_TEXTBOOK;
     int tile = hc.tile;
     if (tile < 0) {
-      // heuristic: 32 x 8 when the blocks are at least 32 wide, else 16 x 16
+      // heuristic: 32 x 8 when the blocks are at least 32 wide, else 16 x 16;
+      // FP64 takes the register-capped 32 x 8 variant
       int64_t minx = 1 << 30;
       for (int b : hc.blocks) minx = std::min(minx, blocks[b].n[0]);
-      tile = (minx >= 32) ? 0 : 1;
+      tile = (minx >= 32) ? (prec == FVM_PREC_FP32_FLUX ? 0 : 2) : 1;
     }
     int gi = -1;
     for (size_t g = 0; g < groups.size(); ++g) {
@@ -465,7 +597,6 @@ int Engine::plan() {
     }
     hc.group = gi;
   }
-  // occupancy per group
   for (auto& G : groups) {
     CK(cudaFuncSetAttribute(G.k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.k.smem));
     int occ = 0;
@@ -473,28 +604,29 @@ int Engine::plan() {
     if (occ < 1) return fail(FVM_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
     G.grid = occ * num_sms;
   }
-  // tasks grouped by kernel, blocks contiguous inside a group
+  // Tasks grouped by kernel; inside a group, longest z range first so the
+  // work queue finishes with the short tasks.
   for (size_t g = 0; g < groups.size(); ++g) {
     Group& G = groups[g];
     G.task_off = (int)tasks.size();
-    // total tile columns of the group for the z-chunk heuristic
-    int64_t cols_planes = 0;
-    for (auto& hc : cases)
-      if (hc.group == (int)g)
-        for (int bi : hc.blocks) {
-          const HBlock& b = blocks[bi];
-          cols_planes += ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty) * b.n[2];
-        }
-    for (auto& hc : cases) {
+    std::vector<Task> gt;
+    for (int ci : live_cases) {
+      HCase& hc = cases[ci];
       if (hc.group != (int)g) continue;
+      // z chunk from the case's own size only, so a case is tiled the same
+      // whether it runs alone or batched with others
+      int64_t cols_planes = 0;
+      for (int bi : hc.blocks) {
+        const HBlock& b = blocks[bi];
+        cols_planes += ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty) * b.n[2];
+      }
       int64_t L = hc.zchunk;
       if (G.dim == 3 && L <= 0) {
         L = (cols_planes + 3 * (int64_t)G.grid - 1) / (3 * (int64_t)G.grid);
         L = std::max<int64_t>(8, round_up(L, 4));
       }
       for (int bi : hc.blocks) {
-        HBlock& b = blocks[bi];
-        block_task0[bi] = (int)tasks.size();
+        const HBlock& b = blocks[bi];
         const int64_t Lb = (G.dim == 3) ? std::min<int64_t>(L, b.n[2]) : b.n[2];
         for (int64_t z0 = 0; z0 < b.n[2]; z0 += Lb)
           for (int64_t y0 = 0; y0 < b.n[1]; y0 += G.k.ty)
@@ -505,14 +637,26 @@ int Engine::plan() {
               t.y0 = (int)y0;
               t.z0 = (int)z0;
               t.z1 = (int)std::min<int64_t>(z0 + Lb, b.n[2]);
-              t.slot = (int)tasks.size();
-              tasks.push_back(t);
+              t.slot = 0;
+              gt.push_back(t);
             }
-        block_ntask[bi] = (int)tasks.size() - block_task0[bi];
       }
     }
+    std::stable_sort(gt.begin(), gt.end(), [](const Task& a, const Task& b) { return (a.z1 - a.z0) > (b.z1 - b.z0); });
+    tasks.insert(tasks.end(), gt.begin(), gt.end());
     G.ntasks = (int)tasks.size() - G.task_off;
     G.grid = std::max(1, std::min(G.grid, G.ntasks));
+  }
+  // partial slots: contiguous per block (the finalize sums a block's slots)
+  {
+    std::vector<std::vector<int>> per_block(blocks.size());
+    for (size_t t = 0; t < tasks.size(); ++t) per_block[tasks[t].blk].push_back((int)t);
+    int slot = 0;
+    for (int bi : live_blocks) {
+      block_task0[bi] = slot;
+      block_ntask[bi] = (int)per_block[bi].size();
+      for (int t : per_block[bi]) tasks[t].slot = slot++;
+    }
   }
   ntasks_total = (int64_t)tasks.size();
 
@@ -528,14 +672,14 @@ int Engine::plan() {
     pairs.push_back(s.slab_off + s.org + y[0] + y[1] * s.sy + y[2] * s.sz);
     return 0;
   };
-  for (size_t bi = 0; bi < blocks.size(); ++bi) {
+  for (int bi : live_blocks) {
     const HBlock& b = blocks[bi];
     for (const auto& c : b.conns)
       for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
         for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j)
           for (int64_t i = c.range[0][0]; i <= c.range[0][1]; ++i) {
             const int64_t x[3] = {i, j, k};
-            if (add_pair((int)bi, x) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
+            if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
           }
     if (cases[b.case_id].cfg.equation == FVM_EQ_NAVIER_STOKES) {
       // layer-1 edge ghosts read by the viscous stencil where both regions are
@@ -552,7 +696,7 @@ int Engine::plan() {
                 x[a] = sa ? b.n[a] : -1;
                 x[a2] = sb ? b.n[a2] : -1;
                 x[c3] = t;
-                if (add_pair((int)bi, x) != 0) return fail(FVM_ERR_INVALID, "edge ghost without a real donor");
+                if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "edge ghost without a real donor");
               }
             }
         }
@@ -560,12 +704,14 @@ int Engine::plan() {
   }
   npairs = (int64_t)pairs.size() / 2;
 
-  // -- device descriptors
+  // -- device descriptors (dead blocks keep an empty descriptor)
   h_dblocks_.assign(blocks.size(), DevBlock());
   for (size_t bi = 0; bi < blocks.size(); ++bi) {
-    const HBlock& b = blocks[bi];
     DevBlock& d = h_dblocks_[bi];
     std::memset(&d, 0, sizeof d);
+    const HBlock& b = blocks[bi];
+    d.case_id = b.case_id;
+    if (b.dead) continue;
     for (int r = 0; r < NROLE; ++r) d.q[r] = role_[r] + b.slab_off + b.org;
     d.rhs = b.rhs_dev;
     d.visc = (visc_ && cases[b.case_id].cfg.equation == FVM_EQ_NAVIER_STOKES) ? visc_ + b.slab_off + b.org : nullptr;
@@ -581,13 +727,11 @@ int Engine::plan() {
     for (int r = 0; r < 6; ++r)
       if (b.bc[r] != FVM_BC_TRANSMISSIVE) mask |= 1 << r;
     d.ghost_mask = mask;
-    d.case_id = b.case_id;
     d.task0 = block_task0[bi];
     d.ntask = block_ntask[bi];
   }
   std::vector<DevCase> hcases(cases.size());
-  std::vector<DevCaseState> hstate(cases.size());
-  int b0 = 0;
+  std::vector<int> case_blk;
   for (size_t ci = 0; ci < cases.size(); ++ci) {
     const fvm_config& c = cases[ci].cfg;
     DevCase& d = hcases[ci];
@@ -608,20 +752,41 @@ int Engine::plan() {
     d.rk_stages = c.rk_stages;
     d.equation = c.equation;
     d.store_rhs = c.store_rhs;
-    // blocks of a case are contiguous in creation order only if added so;
-    // the finalize walks [block0, block0+nblocks), so require it.
-    d.block0 = cases[ci].blocks.empty() ? 0 : cases[ci].blocks.front();
+    d.block0 = (int)case_blk.size();
+    d.nblocks = 0;
+    if (cases[ci].dead) continue;
+    for (int b : cases[ci].blocks) case_blk.push_back(b);
     d.nblocks = (int)cases[ci].blocks.size();
-    for (int k = 0; k < d.nblocks; ++k)
-      if (cases[ci].blocks[k] != d.block0 + k) return fail(FVM_ERR_INVALID, "blocks of a case must be added contiguously");
-    b0 += d.nblocks;
-    std::memset(&hstate[ci], 0, sizeof(DevCaseState));
-    hstate[ci].dt = c.dt;
   }
-  (void)b0;
+  // per-case evolving state: kept across re-plans, initialised for new cases
+  if (state_cap_ < (int)cases.size()) {
+    const int ncap = std::max<int>(64, (int)cases.size() * 2);
+    DevCaseState* ns = nullptr;
+    CK(cudaMalloc(&ns, sizeof(DevCaseState) * ncap));
+    CK(cudaMemsetAsync(ns, 0, sizeof(DevCaseState) * ncap, stream));
+    if (d_state_) {
+      CK(cudaMemcpyAsync(ns, d_state_, sizeof(DevCaseState) * state_cap_, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaStreamSynchronize(stream));
+      cudaFree(d_state_);
+    }
+    d_state_ = ns;
+    state_cap_ = ncap;
+  }
+  for (int ci : live_cases) {
+    if (!cases[ci].fresh) continue;
+    DevCaseState s;
+    std::memset(&s, 0, sizeof s);
+    s.dt = cases[ci].cfg.dt;
+    CK(cudaMemcpyAsync(d_state_ + ci, &s, sizeof s, cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    cases[ci].fresh = false;
+  }
+  void* old[] = {d_blocks_, d_cases_, d_case_blk_, d_tasks_, d_partials_, d_pairs_, d_counters_, d_casemax_};
+  for (void* p : old)
+    if (p) cudaFree(p);
   CK(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks.size()));
   CK(cudaMalloc(&d_cases_, sizeof(DevCase) * cases.size()));
-  CK(cudaMalloc(&d_state_, sizeof(DevCaseState) * cases.size()));
+  CK(cudaMalloc(&d_case_blk_, sizeof(int) * std::max<size_t>(1, case_blk.size())));
   CK(cudaMalloc(&d_tasks_, sizeof(Task) * std::max<size_t>(1, tasks.size())));
   CK(cudaMalloc(&d_partials_, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size())));
   CK(cudaMalloc(&d_pairs_, sizeof(int64_t) * std::max<size_t>(2, pairs.size())));
@@ -630,7 +795,8 @@ int Engine::plan() {
   CK(cudaMalloc(&d_casemax_, sizeof(unsigned long long) * cases.size()));
   CK(cudaMemcpyAsync(d_blocks_, h_dblocks_.data(), sizeof(DevBlock) * blocks.size(), cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_cases_, hcases.data(), sizeof(DevCase) * cases.size(), cudaMemcpyHostToDevice, stream));
-  CK(cudaMemcpyAsync(d_state_, hstate.data(), sizeof(DevCaseState) * cases.size(), cudaMemcpyHostToDevice, stream));
+  if (!case_blk.empty())
+    CK(cudaMemcpyAsync(d_case_blk_, case_blk.data(), sizeof(int) * case_blk.size(), cudaMemcpyHostToDevice, stream));
   if (!tasks.empty())
     CK(cudaMemcpyAsync(d_tasks_, tasks.data(), sizeof(Task) * tasks.size(), cudaMemcpyHostToDevice, stream));
   if (!pairs.empty())
@@ -649,8 +815,12 @@ int Engine::plan() {
 // kind of each launch (1 stage, 2 gather, 3 viscous, 4 finalize) returned.
 int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
   bool any_ns = false;
-  for (auto& c : cases) any_ns |= c.cfg.equation == FVM_EQ_NAVIER_STOKES;
+  for (auto& c : cases)
+    if (!c.dead) any_ns |= c.cfg.equation == FVM_EQ_NAVIER_STOKES;
   const int S = max_stages_;
+  // groups run as parallel branches of the captured graph (fork / join on
+  // side streams); the profiled path launches them in sequence to time each
+  const bool fork = (evs == nullptr) && groups.size() > 1;
   int n = 0;
   auto mark = [&](int kind) -> cudaError_t {
     if (evs && n < nev) {
@@ -663,6 +833,7 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
     return cudaSuccess;
   };
   if (evs && nev > 0) CK(cudaEventRecord(evs[0], stream));
+  int ev_i = 0;
   for (int m = 1; m <= S; ++m) {
     int rin, rout;
     stage_roles(S, m, &rin, &rout);
@@ -670,6 +841,8 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
       CK(launch_visc(d_blocks_, (int)blocks.size(), d_cases_, rin, stream));
       CK(mark(3));
     }
+    if (fork) CK(cudaEventRecord(fork_ev_[ev_i], stream));
+    const int fork_ev = ev_i++;
     for (size_t g = 0; g < groups.size(); ++g) {
       const Group& G = groups[g];
       StageArgs a;
@@ -687,7 +860,17 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
       a.racc = (S == 4) ? ROLE_ACC : ROLE_A;
       a.last = (m == S) ? 1 : 0;
       void* args[] = {&a};
-      CK(cudaLaunchKernel(G.k.fn, dim3(G.grid), dim3(G.k.threads), args, G.k.smem, stream));
+      cudaStream_t st = stream;
+      if (fork) {
+        st = side_[g];
+        CK(cudaStreamWaitEvent(st, fork_ev_[fork_ev], 0));
+      }
+      CK(cudaLaunchKernel(G.k.fn, dim3(G.grid), dim3(G.k.threads), args, G.k.smem, st));
+      if (fork) {
+        CK(cudaEventRecord(fork_ev_[ev_i], st));
+        CK(cudaStreamWaitEvent(stream, fork_ev_[ev_i], 0));
+        ++ev_i;
+      }
       CK(mark(1));
     }
     if (npairs > 0) {
@@ -695,7 +878,8 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
       CK(mark(2));
     }
   }
-  CK(launch_finalize(d_blocks_, d_cases_, d_state_, (int)cases.size(), d_partials_, d_counters_, ncounters_, stream));
+  CK(launch_finalize(d_blocks_, d_cases_, d_case_blk_, d_state_, (int)cases.size(), d_partials_, d_counters_,
+                     ncounters_, stream));
   CK(mark(4));
   if (nlaunch) *nlaunch = n;
   return FVM_OK;
@@ -706,6 +890,17 @@ int Engine::build_graph() {
   if (graph_) cudaGraphDestroy(graph_);
   gexec_ = nullptr;
   graph_ = nullptr;
+  while (side_.size() < groups.size()) {
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    side_.push_back(st);
+  }
+  const size_t nev = (size_t)max_stages_ * (groups.size() + 1);
+  while (fork_ev_.size() < nev) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    fork_ev_.push_back(e);
+  }
   CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
   int launches = 0;
   int rc = enqueue_step(nullptr, 0, nullptr, &launches);
@@ -759,7 +954,7 @@ int Engine::prepare() {
 
 // ---------------------------------------------------------------- state
 int Engine::set_state(int blk, const double* q) {
-  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!q) return fail(FVM_ERR_INVALID, "null state");
   int rc = ensure_planned();
   if (rc) return rc;
@@ -774,9 +969,13 @@ int Engine::set_state(int blk, const double* q) {
 }
 
 int Engine::get_state(int blk, double* q, int prim) {
-  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!q) return fail(FVM_ERR_INVALID, "null output");
-  if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
+  if (!planned_) {
+    if (cap_ == 0) return fail(FVM_ERR_STATE, "no state uploaded yet");
+    int rc = plan();
+    if (rc) return rc;
+  }
   const HBlock& b = blocks[blk];
   const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
   CK(launch_pack(h_dblocks_[blk].q[ROLE_A], cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
@@ -787,7 +986,7 @@ int Engine::get_state(int blk, double* q, int prim) {
 }
 
 int Engine::get_rhs(int blk, double* rhs) {
-  if (blk < 0 || blk >= (int)blocks.size()) return fail(FVM_ERR_INVALID, "bad block id");
+  if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!rhs) return fail(FVM_ERR_INVALID, "null output");
   const HBlock& b = blocks[blk];
   if (!cases[b.case_id].cfg.store_rhs) return fail(FVM_ERR_STATE, "store_rhs is off");
@@ -800,7 +999,11 @@ int Engine::get_rhs(int blk, double* rhs) {
 
 int Engine::step(int nsteps) {
   if (nsteps < 0) return fail(FVM_ERR_INVALID, "nsteps < 0");
-  if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
+  if (!planned_) {
+    if (cap_ == 0) return fail(FVM_ERR_STATE, "no state uploaded yet");
+    int rc = plan();
+    if (rc) return rc;
+  }
   if (!prepared_) {
     int rc = prepare();
     if (rc) return rc;
@@ -810,6 +1013,7 @@ int Engine::step(int nsteps) {
 }
 
 int Engine::read_case_state(int case_id, DevCaseState* out) {
+  if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
   if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
   CK(cudaMemcpyAsync(out, d_state_ + case_id, sizeof(DevCaseState), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
@@ -937,6 +1141,12 @@ int fvm_step(fvm_ctx* ctx, int nsteps, double* t, double* res_abs, double* res_r
   if (!ctx) return FVM_ERR_INVALID;
   int rc = ctx->eng.step(nsteps);
   if (rc) return rc;
+  if (!ctx->eng.live_case(ctx->case_id)) {
+    // the context's first case was removed (a batch / serving engine): no
+    // outputs to report, but keep the call synchronous
+    const cudaError_t e = cudaStreamSynchronize(ctx->eng.stream);
+    return e == cudaSuccess ? FVM_OK : ctx->eng.cuda_fail(e, "fvm_step");
+  }
   fvm::DevCaseState s;
   rc = ctx->eng.read_case_state(ctx->case_id, &s);
   if (rc) return rc;
@@ -1003,6 +1213,50 @@ int fvm_last_error(const fvm_ctx* ctx, char* buf, size_t n) {
   if (!buf || n == 0) return FVM_ERR_INVALID;
   const std::string& m = ctx ? ctx->eng.err : g_create_error;
   std::snprintf(buf, n, "%s", m.c_str());
+  return FVM_OK;
+}
+
+int fvm_reserve(fvm_ctx* ctx, int64_t cells) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.reserve(cells);
+}
+
+int fvm_block_cells(int idimension, const int64_t nvert[3], int64_t* cells) {
+  if (!nvert || !cells || (idimension != 2 && idimension != 3)) return FVM_ERR_INVALID;
+  for (int d = 0; d < 3; ++d)
+    if (nvert[d] < 1) return FVM_ERR_INVALID;
+  *cells = fvm::padded_cells(idimension, nvert);
+  return FVM_OK;
+}
+
+int fvm_add_case(fvm_ctx* ctx, const fvm_config* cfg, int* case_id) {
+  if (!ctx || !cfg) return FVM_ERR_INVALID;
+  return ctx->eng.add_case(*cfg, case_id);
+}
+
+int fvm_add_case_block(fvm_ctx* ctx, int case_id, const int64_t nvert[3], const double dr[3], int* blk) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.add_block(case_id, nvert, dr, blk);
+}
+
+int fvm_remove_case(fvm_ctx* ctx, int case_id) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.remove_case(case_id);
+}
+
+int fvm_case_state(fvm_ctx* ctx, int case_id, double* t, double* dt, int64_t* step, double* res_abs,
+                   double* res_rel, int* status) {
+  if (!ctx) return FVM_ERR_INVALID;
+  fvm::DevCaseState s;
+  std::memset(&s, 0, sizeof s);
+  int rc = ctx->eng.read_case_state(case_id, &s);
+  if (rc) return rc;
+  if (t) *t = s.t;
+  if (dt) *dt = s.dt_last;
+  if (step) *step = s.step;
+  if (res_abs) std::memcpy(res_abs, s.res_abs, sizeof s.res_abs);
+  if (res_rel) std::memcpy(res_rel, s.res_rel, sizeof s.res_rel);
+  if (status) *status = s.status;
   return FVM_OK;
 }
 

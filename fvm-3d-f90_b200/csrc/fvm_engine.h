@@ -1,16 +1,23 @@
-// fvm_engine.h — host runtime: blocks, cases, HBM layout, work lists, ghost
-// gather lists and the captured CUDA graph of one time step.
+// fvm_engine.h — host runtime: cases, blocks, the HBM arena, work lists,
+// ghost gather lists and the captured CUDA graph of one time step.
 //
-// One Engine advances any number of cases (each a set of blocks with its own
-// scheme configuration) in lockstep: every RK stage is one persistent launch
-// per scheme group over the tile work list, followed by the ghost gather; a
-// finalize kernel closes the step (residuals, time, next dt). The whole step
-// is captured once into a CUDA graph and replayed.
+// One Engine advances any number of independent cases (each a set of blocks
+// with its own scheme configuration) in lockstep: every RK stage is one
+// persistent launch per scheme group over the tile work list (groups run as
+// parallel graph branches), followed by the ghost gather; a finalize kernel
+// closes the step (per-case residuals, time, next dt). The step is captured
+// once into a CUDA graph and replayed.
+//
+// State lives in a persistent arena: one slab per (role, variable) whose
+// blocks get ranges from a first-fit allocator. Cases can be added and
+// removed between steps (the serving loop does this); re-planning rebuilds
+// descriptors, tasks and the graph but never moves or clears live state.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/fvm3d.h"
@@ -28,14 +35,17 @@ struct HConn {
 
 struct HBlock {
   int case_id = 0;
+  bool dead = false;
+  bool fresh = true;     // region not yet cleared in the arena
   int64_t n[3] = {1, 1, 1};
   double dr[3] = {1, 1, 1};
   int bc[6] = {0, 0, 0, 0, 0, 0};
   std::vector<HConn> conns;
-  // layout (set by plan)
+  // layout
   int64_t px = 0, py = 0, pz = 0, zpad = 0;
-  int64_t slab_off = 0;  // element offset of the block's padded box in a slab
-  int64_t org = 0;       // element offset of real cell (0,0,0) in a slab
+  int64_t padded = 0;     // elements of the padded box in one variable slab
+  int64_t slab_off = -1;  // element offset of the padded box, -1 = unassigned
+  int64_t org = 0;        // offset of real cell (0,0,0) inside the padded box
   int64_t sy = 0, sz = 0;
   double* rhs_dev = nullptr;
 };
@@ -43,6 +53,8 @@ struct HBlock {
 struct HCase {
   fvm_config cfg;
   std::vector<int> blocks;
+  bool dead = false;
+  bool fresh = true;    // device state (time, residual history) not initialised
   int group = -1;
   int tile = -1;        // forced tile (autotuner result), -1 = heuristic
   int zchunk = 0;       // forced z chunk, 0 = heuristic
@@ -56,15 +68,20 @@ struct Group {
   int grid = 0;
 };
 
+// Padded arena elements one block of this shape occupies in one variable slab.
+int64_t padded_cells(int idimension, const int64_t n[3]);
+
 class Engine {
  public:
   Engine();
   ~Engine();
 
-  int add_case(const fvm_config& cfg);
+  int add_case(const fvm_config& cfg, int* case_id = nullptr);
+  int remove_case(int case_id);
   int add_block(int case_id, const int64_t n[3], const double dr[3], int* blk);
   int set_boundary(int blk, int region, int kind);
   int connect(int blk, const int64_t range[3][2], int donor, const int64_t drange[3][2], const int32_t dtype[3]);
+  int reserve(int64_t cells);
 
   int set_state(int blk, const double* q);
   int get_state(int blk, double* q, int prim);
@@ -74,7 +91,7 @@ class Engine {
 
   // Tuning hooks (autotuner): force tile shape / z chunk of a case.
   int set_tuning(int case_id, int tile, int zchunk);
-  // Time one stage launch of every group (ms), for the autotuner.
+  // Mean device time of `reps` graph-launched steps (ms).
   int time_stage(int reps, float* ms);
 
   std::string err;
@@ -94,27 +111,41 @@ class Engine {
   }
   int cuda_fail(cudaError_t e, const char* where);
   int ensure_planned();
-  int prepare();  // gather ghosts of role A + initial dt, after state uploads
+  int prepare();  // gather ghosts of role A + dt of every case, after state uploads
   int profile_step(float* ms, int* kinds, int cap, int* n);
+  int live_case(int case_id) const {
+    return case_id >= 0 && case_id < (int)cases.size() && !cases[case_id].dead;
+  }
+  int live_block(int blk) const { return blk >= 0 && blk < (int)blocks.size() && !blocks[blk].dead; }
 
  private:
   int plan();
   int build_graph();
   int enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch);
-  void release();
+  void release();      // free everything (destruction)
+  void invalidate() {  // topology changed: re-plan before the next use
+    planned_ = false;
+    prepared_ = false;
+  }
+  int alloc_range(int64_t size, int64_t* off);
+  void free_range(int64_t off, int64_t size);
+  int grow_arena(int64_t need);
   int resolve(int blk, int64_t x[3], int* out_blk) const;
 
   bool planned_ = false;
   bool prepared_ = false;
   int nroles_ = 3;
   int max_stages_ = 3;
-  int64_t cap_ = 0;
+  int64_t cap_ = 0;            // elements per variable slab (0 = no arena yet)
+  int64_t reserved_ = 0;       // fixed arena size requested by reserve()
+  std::vector<std::pair<int64_t, int64_t>> free_;  // (offset, size), sorted
   double* role_[NROLE] = {nullptr, nullptr, nullptr, nullptr};
   double* visc_ = nullptr;
-  double* rhs_all_ = nullptr;
   DevBlock* d_blocks_ = nullptr;
   DevCase* d_cases_ = nullptr;
+  int* d_case_blk_ = nullptr;
   DevCaseState* d_state_ = nullptr;
+  int state_cap_ = 0;
   Task* d_tasks_ = nullptr;
   double* d_partials_ = nullptr;
   int64_t* d_pairs_ = nullptr;
@@ -125,6 +156,8 @@ class Engine {
   size_t staging_bytes_ = 0;
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
+  std::vector<cudaStream_t> side_;  // fork streams for parallel group launches
+  std::vector<cudaEvent_t> fork_ev_;
   std::vector<DevBlock> h_dblocks_;
 };
 

@@ -49,7 +49,7 @@ struct DevCase {
   int32_t idim;
   int32_t rk_stages;
   int32_t nblocks;
-  int32_t block0;              // first block of the case in the engine block table
+  int32_t block0;              // first entry of the case in the case-block index list
   int32_t equation;
   int32_t store_rhs;
   int32_t pad_;

@@ -171,6 +171,13 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "fvm_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
         "fvm_destroy": (ctypes.c_int, [vp]),
         "fvm_residual_norms": (ctypes.c_int, [vp, P(i64), vp, vp]),
+        "fvm_reserve": (ctypes.c_int, [vp, i64]),
+        "fvm_block_cells": (ctypes.c_int, [ctypes.c_int, P(i64), P(i64)]),
+        "fvm_add_case": (ctypes.c_int, [vp, P(FvmConfig), P(ctypes.c_int)]),
+        "fvm_add_case_block": (ctypes.c_int, [vp, ctypes.c_int, P(i64), P(dbl), P(ctypes.c_int)]),
+        "fvm_remove_case": (ctypes.c_int, [vp, ctypes.c_int]),
+        "fvm_case_state": (ctypes.c_int, [vp, ctypes.c_int, P(dbl), P(dbl), P(i64), P(dbl), P(dbl),
+                                          P(ctypes.c_int)]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)
@@ -179,6 +186,22 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
     if path is None:
         _lib = lib
     return lib
+
+
+def block_cells(idimension: int, nvert) -> int:
+    """Arena cells (per variable slab) a block of this shape occupies."""
+    lib = load_library()
+    out = ctypes.c_int64()
+    rc = lib.fvm_block_cells(int(idimension), (ctypes.c_int64 * 3)(*[int(x) for x in nvert]), ctypes.byref(out))
+    if rc != 0:
+        raise ValueError(f"fvm_block_cells failed ({rc})")
+    return out.value
+
+
+def block_bytes(cfg: FvmConfig, nvert) -> int:
+    """Device bytes the state of one block takes (all RK roles, viscous slab)."""
+    slabs = (4 if cfg.rk_stages == 4 else 3) + (1 if cfg.equation == EQ_NAVIER_STOKES else 0)
+    return block_cells(cfg.idimension, nvert) * 5 * 8 * slabs
 
 
 def declared_symbols(header: str) -> list[str]:

@@ -69,16 +69,21 @@ class Case:
         d.update(over)
         return abi.make_config(**d)
 
-    def apply(self, target, states: bool = True):
+    def apply(self, target, states: bool = True, case_id: int | None = None):
+        """Replay the case on `target`. With case_id, the blocks go to that
+        case of a multi-case Solver and the engine's block ids are kept in
+        self.block_ids (local block b -> engine block id)."""
+        ids = []
         for n, dr in self.blocks:
-            target.add_block(n, dr)
+            ids.append(target.add_block(n, dr) if case_id is None else target.add_case_block(case_id, n, dr))
+        self.block_ids = ids
         for blk, region, kind in self.bcs:
-            target.set_boundary(blk, region, kind)
+            target.set_boundary(ids[blk], region, kind)
         for blk, rng, donor, drng, dtype in self.conns:
-            target.connect(blk, rng, donor, drng, dtype)
+            target.connect(ids[blk], rng, ids[donor], drng, dtype)
         if states:
             for b, q in enumerate(self.states):
-                target.set_state(b, q)
+                target.set_state(ids[b], q)
         return target
 
 

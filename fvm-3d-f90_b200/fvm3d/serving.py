@@ -1,0 +1,203 @@
+"""Serving loop: continuous batching of solver requests on one GPU.
+
+Requests (a seeded case plus a number of RK steps) arrive over time. The
+server keeps every admitted case's state resident in one engine whose state
+arena is reserved up front (the HBM budget); a request is admitted, first come
+first served, as soon as its blocks fit into the free arena, and it joins the
+running batch at the next step boundary: all admitted cases advance together,
+one persistent launch per stage. A finished case is read back and removed,
+which frees its arena range for the queue. Time-to-solution is measured from
+arrival to the moment its final state is on the host.
+
+The one-at-a-time baseline serves the same stream in arrival order with one
+engine per request.
+
+The engine keeps a case's tiling, time step and residual sums independent of
+its neighbours, so a case's final state is the same alone and in the mix.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi, cases
+from .solver import FvmError, Solver
+
+
+@dataclass
+class Request:
+    rid: int
+    case: cases.Case
+    nsteps: int
+    arrival: float                # seconds after the stream starts
+    cells: int = 0                # arena cells the request needs
+    case_id: int = -1
+    remaining: int = 0
+    admitted: float = math.nan
+    finished: float = math.nan
+    result: list = field(default_factory=list)
+    status: int = 0
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+    @property
+    def work(self) -> int:
+        """cell-stage updates the request asks for"""
+        return self.case.ncells * int(self.case.cfg.get("rk_stages", 3)) * self.nsteps
+
+
+def poisson_stream(n: int, rate: float, seed: int, make_case, steps=(200, 2000)):
+    """n requests with exponential inter-arrival times (mean 1/rate seconds);
+    make_case(rng, i) builds the i-th case; step counts uniform in `steps`."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        c = make_case(rng, i)
+        out.append(Request(rid=i, case=c, nsteps=int(rng.integers(steps[0], steps[1] + 1)), arrival=t))
+    return out
+
+
+def mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(32, 96)):
+    """Case builder for the serving stream: blasts and oblique shock tubes of
+    random cube size, random Roe / AUSM and MUSCL / WENO5, SSP-RK3."""
+    def make(rng, i):
+        n = int(round(sizes[0] * (sizes[1] / sizes[0]) ** rng.uniform()))
+        n = max(8, n)
+        recon = [abi.RECON_MUSCL, abi.RECON_WENO][int(rng.integers(2))]
+        flux = [abi.FLUX_ROE, abi.FLUX_AUSM][int(rng.integers(2))]
+        fam = cases.blast if rng.uniform() < 0.5 else cases.shock_tube
+        return fam((n, n, n), seed=int(rng.integers(1 << 30)), reconstruct=recon, flux_split=flux,
+                   limiter=abi.LIMITER_MINMOD, kappa=1.0 / 3.0, precision=precision, rk_stages=3)
+    return make
+
+
+class Server:
+    """Continuous-batching server over one engine with a fixed state arena."""
+
+    def __init__(self, budget_cells: int, rk_stages: int = 3, chunk: int = 16):
+        # the context's own first case is only a placeholder for the engine
+        self.s = Solver(abi.make_config(rk_stages=rk_stages))
+        self.s.remove_case(0)
+        self.s.reserve(budget_cells)
+        self.budget = budget_cells
+        self.free = budget_cells
+        self.chunk = chunk
+        self.active: list[Request] = []
+        self.steps_run = 0
+
+    def close(self):
+        self.s.close()
+
+    def cells_of(self, c: cases.Case) -> int:
+        idim = int(c.cfg.get("idimension", 3))
+        return sum(abi.block_cells(idim, n) for n, _ in c.blocks)
+
+    def fits(self, r: Request) -> bool:
+        return r.cells <= self.free
+
+    def admit(self, r: Request, now: float) -> bool:
+        """Place the request's blocks in the arena and upload its state; on a
+        fragmented arena (enough cells in total, no contiguous range) the case
+        is taken out again and the request stays queued."""
+        cid = self.s.add_case(r.case.config())
+        try:
+            r.case.apply(self.s, case_id=cid)
+        except FvmError as e:
+            if e.code != 3:  # FVM_ERR_NOMEM
+                raise
+            self.s.remove_case(cid)
+            return False
+        r.case_id = cid
+        r.remaining = r.nsteps
+        r.admitted = now
+        self.free -= r.cells
+        self.active.append(r)
+        return True
+
+    def retire(self, r: Request, now: float):
+        r.result = [self.s.get_state(b) for b in r.case.block_ids]
+        r.status = self.s.case_state(r.case_id)["status"]
+        self.s.remove_case(r.case_id)
+        self.free += r.cells
+        r.finished = now
+        self.active.remove(r)
+
+    def run(self, stream: list[Request], clock=time.perf_counter, realtime: bool = True):
+        """Serve the stream; arrivals are honoured in wall-clock time when
+        `realtime`, else every request is present at t = 0. Returns stats."""
+        pending = sorted(stream, key=lambda r: r.arrival)
+        for r in pending:
+            r.cells = self.cells_of(r.case)
+            if r.cells > self.budget:
+                raise ValueError(f"request {r.rid} needs {r.cells} cells, more than the whole budget")
+        queue: list[Request] = []
+        done: list[Request] = []
+        t0 = clock()
+        i = 0
+        while i < len(pending) or queue or self.active:
+            now = clock() - t0
+            while i < len(pending) and (not realtime or pending[i].arrival <= now):
+                queue.append(pending[i])
+                i += 1
+            while queue and self.fits(queue[0]):
+                if not self.admit(queue[0], now):
+                    break
+                queue.pop(0)
+            if not self.active:
+                if queue:
+                    raise RuntimeError("a queued request cannot be placed in the empty arena")
+                if i < len(pending) and realtime:
+                    time.sleep(max(0.0, min(0.002, pending[i].arrival - now)))
+                continue
+            k = min(min(r.remaining for r in self.active), self.chunk)
+            self.s.step(k)
+            self.steps_run += k
+            now = clock() - t0
+            for r in list(self.active):
+                r.remaining -= k
+                if r.remaining == 0:
+                    self.retire(r, clock() - t0)
+                    done.append(r)
+        makespan = clock() - t0
+        return summarize(done, makespan)
+
+
+def serve_one_at_a_time(stream: list[Request], clock=time.perf_counter, realtime: bool = True):
+    """Baseline: one engine per request, strictly in arrival order."""
+    pending = sorted(stream, key=lambda r: r.arrival)
+    done = []
+    t0 = clock()
+    for r in pending:
+        now = clock() - t0
+        if realtime and r.arrival > now:
+            time.sleep(r.arrival - now)
+        r.admitted = clock() - t0
+        s = r.case.apply(Solver(r.case.config()))
+        s.step(r.nsteps)
+        r.result = [s.get_state(b) for b in range(len(r.case.blocks))]
+        r.status = s.case_state(0)["status"]
+        s.close()
+        r.finished = clock() - t0
+        done.append(r)
+    return summarize(done, clock() - t0)
+
+
+def summarize(done: list[Request], makespan: float) -> dict:
+    lat = np.array([r.latency for r in done]) if done else np.zeros(1)
+    work = float(sum(r.work for r in done))
+    return {
+        "requests": len(done),
+        "p50_s": float(np.percentile(lat, 50)),
+        "p99_s": float(np.percentile(lat, 99)),
+        "mean_s": float(lat.mean()),
+        "makespan_s": makespan,
+        "gcell_stage_per_s": work / makespan / 1e9 if makespan > 0 else 0.0,
+        "failed": int(sum(1 for r in done if r.status != 0)),
+    }

@@ -73,7 +73,9 @@ class Solver:
         d = (ctypes.c_double * 3)(*[float(x) for x in dr])
         b = ctypes.c_int()
         self._chk(self.lib.fvm_add_block(self.h, n, d, ctypes.byref(b)))
-        self.shapes.append(tuple(int(x) for x in nvert))
+        while len(self.shapes) <= b.value:
+            self.shapes.append(None)
+        self.shapes[b.value] = tuple(int(x) for x in nvert)
         return b.value
 
     def set_boundary(self, blk: int, region: int, kind: int):
@@ -84,6 +86,42 @@ class Solver:
         d = (ctypes.c_int64 * 6)(*[int(x) for pair in drng for x in pair])
         t = (ctypes.c_int32 * 3)(*[int(x) for x in dtype])
         self._chk(self.lib.fvm_connect(self.h, blk, r, donor, d, t))
+
+    # -- batched / served cases
+    def reserve(self, cells: int):
+        """Fix the state arena at `cells` padded cells per variable slab."""
+        self._chk(self.lib.fvm_reserve(self.h, int(cells)))
+
+    def add_case(self, cfg: abi.FvmConfig | None = None, **kw) -> int:
+        c = cfg if cfg is not None else abi.make_config(**kw)
+        cid = ctypes.c_int()
+        self._chk(self.lib.fvm_add_case(self.h, ctypes.byref(c), ctypes.byref(cid)))
+        return cid.value
+
+    def add_case_block(self, case_id: int, nvert, dr) -> int:
+        n = (ctypes.c_int64 * 3)(*[int(x) for x in nvert])
+        d = (ctypes.c_double * 3)(*[float(x) for x in dr])
+        b = ctypes.c_int()
+        self._chk(self.lib.fvm_add_case_block(self.h, int(case_id), n, d, ctypes.byref(b)))
+        while len(self.shapes) <= b.value:
+            self.shapes.append(None)
+        self.shapes[b.value] = tuple(int(x) for x in nvert)
+        return b.value
+
+    def remove_case(self, case_id: int):
+        self._chk(self.lib.fvm_remove_case(self.h, int(case_id)))
+
+    def case_state(self, case_id: int) -> dict:
+        t = ctypes.c_double()
+        dt = ctypes.c_double()
+        st = ctypes.c_int64()
+        ra = np.zeros(6)
+        rr = np.zeros(6)
+        status = ctypes.c_int()
+        self._chk(self.lib.fvm_case_state(self.h, int(case_id), ctypes.byref(t), ctypes.byref(dt),
+                                          ctypes.byref(st), _dp(ra), _dp(rr), ctypes.byref(status)))
+        return {"t": t.value, "dt": dt.value, "step": st.value, "res_abs": ra, "res_rel": rr,
+                "status": status.value}
 
     # -- state
     def set_state(self, blk: int, q: np.ndarray):

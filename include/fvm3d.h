@@ -193,6 +193,33 @@ int fvm_get_time(fvm_ctx* ctx, double* t, double* dt, int64_t* step);
  * ctx is NULL) into buf (NUL-terminated, truncated to n bytes). */
 int fvm_last_error(const fvm_ctx* ctx, char* buf, size_t n);
 
+/* ---- batched and served cases (no counterpart in the reference, which runs
+ *      one case per process) ------------------------------------------------
+ * A context can hold many independent cases; fvm_step advances all of them in
+ * lockstep (blocks of every case share each persistent stage launch), while
+ * fvm_step's own t / residual outputs and error refer to the context's first
+ * case. Cases can be added and removed between steps without touching the
+ * state of the others. */
+
+/* Fix the size of the state arena (padded cells per variable, the sum of
+ * fvm_block_cells over the blocks it must hold) before the first upload: the
+ * HBM budget of a served engine. Without it the arena holds exactly the
+ * blocks present and grows when more are added. */
+int fvm_reserve(fvm_ctx* ctx, int64_t cells);
+/* Arena cells one block of this shape takes; its device bytes are
+ * cells * 5 * 8 * (3 for SSP-RK3, 4 for RK4), +1 slab for Navier-Stokes. */
+int fvm_block_cells(int idimension, const int64_t nvert[3], int64_t* cells);
+/* Add a case with its own configuration (same rk_stages as the others). */
+int fvm_add_case(fvm_ctx* ctx, const fvm_config* cfg, int* case_id);
+/* fvm_add_block for a given case; block ids are unique across cases. */
+int fvm_add_case_block(fvm_ctx* ctx, int case_id, const int64_t nvert[3], const double dr[3], int* blk);
+/* Remove a case and free its arena ranges. */
+int fvm_remove_case(fvm_ctx* ctx, int case_id);
+/* Time, last dt, step count, residuals and status (FVM_OK, FVM_ERR_NONFINITE,
+ * FVM_ERR_DIVERGED) of one case. Any pointer may be NULL. */
+int fvm_case_state(fvm_ctx* ctx, int case_id, double* t, double* dt, int64_t* step, double* res_abs,
+                   double* res_rel, int* status);
+
 /* Autotuner hooks; no counterpart in the reference. fvm_tune_set forces the
  * tile shape (index 0: 32x8, 1: 16x16, 2: 32x8 with registers capped for two
  * resident CTAs per SM; -1 = heuristic) and z chunk length

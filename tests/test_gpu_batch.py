@@ -1,0 +1,102 @@
+"""Batched cases in one engine and the continuous-batching server."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from fvm3d import abi, cases, serving
+from fvm3d.solver import FvmError, Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def alone(case, steps):
+    s = case.apply(Solver(case.config()))
+    s.step(steps)
+    out = [s.get_state(b) for b in range(len(case.blocks))]
+    s.close()
+    return out
+
+
+def trio():
+    a = cases.blast((24, 20, 16), seed=1, reconstruct=abi.RECON_MUSCL, flux_split=abi.FLUX_ROE,
+                    limiter=abi.LIMITER_MINMOD, kappa=1.0 / 3.0)
+    b = cases.shock_tube((16, 24, 20), seed=2, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM)
+    c = cases.isentropic_vortex(N=16, layout="blocks8", rk_stages=3, reconstruct=abi.RECON_SIMPLE,
+                                flux_split=abi.FLUX_VANLEER)
+    return [a, b, c]
+
+
+def test_batch_equals_alone_and_oracle():
+    cs = trio()
+    s = Solver(cs[0].config())
+    s.remove_case(0)
+    ids = []
+    for c in cs:
+        cid = s.add_case(c.config())
+        c.apply(s, case_id=cid)
+        ids.append(list(c.block_ids))
+    s.step(4)
+    for c, bid in zip(cs, ids):
+        ref = alone(c, 4)
+        o = c.apply(orc.Oracle(c.config()))
+        o.step(4)
+        for b, g in enumerate(bid):
+            got = s.get_state(g)
+            assert np.array_equal(got, ref[b])
+            assert np.array_equal(got, o.get_state(b))
+    s.close()
+
+
+def test_add_and_remove_between_steps():
+    a, b, c = trio()
+    s = Solver(a.config())
+    s.remove_case(0)
+    ca = s.add_case(a.config())
+    a.apply(s, case_id=ca)
+    cb = s.add_case(b.config())
+    b.apply(s, case_id=cb)
+    ids_b = list(b.block_ids)
+    s.step(3)
+    s.remove_case(ca)
+    cc = s.add_case(c.config())
+    c.apply(s, case_id=cc)
+    ids_c = list(c.block_ids)
+    s.step(2)
+    ref_b = alone(b, 5)
+    ref_c = alone(c, 2)
+    for i, g in enumerate(ids_b):
+        assert np.array_equal(s.get_state(g), ref_b[i])
+    for i, g in enumerate(ids_c):
+        assert np.array_equal(s.get_state(g), ref_c[i])
+    assert s.case_state(cb)["step"] == 5 and s.case_state(cc)["step"] == 2
+    s.close()
+
+
+def test_reserved_budget_is_enforced():
+    a, b, _ = trio()
+    need = sum(abi.block_cells(3, n) for n, _ in a.blocks)
+    s = Solver(a.config())
+    s.remove_case(0)
+    s.reserve(need)
+    ca = s.add_case(a.config())
+    a.apply(s, case_id=ca)
+    cb = s.add_case(b.config())
+    with pytest.raises(FvmError) as e:
+        b.apply(s, case_id=cb)  # the upload plans the arena: no room
+    assert e.value.code == 3
+    s.close()
+
+
+def test_server_results_same_alone_and_in_the_mix():
+    make = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(12, 24))
+    stream = serving.poisson_stream(8, rate=1000.0, seed=3, make_case=make, steps=(3, 12))
+    budget = 3 * max(sum(abi.block_cells(3, n) for n, _ in r.case.blocks) for r in stream)
+    srv = serving.Server(budget_cells=budget, chunk=4)
+    stats = srv.run(stream, realtime=False)
+    srv.close()
+    assert stats["requests"] == 8 and stats["failed"] == 0
+    assert stats["p99_s"] >= stats["p50_s"] > 0
+    for r in stream:
+        ref = alone(r.case, r.nsteps)
+        for got, want in zip(r.result, ref):
+            assert np.array_equal(got, want), f"request {r.rid}"
