@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--n", type=int, default=128, help="global grid edge (cells)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-case batched leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--batch-cases", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--tile", type=int, default=None, help="fixed tile index (skips the autotuner)")
     ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk with --tile")
     ap.add_argument("--forms", default="fp32,fp64,exact",
@@ -293,6 +297,84 @@ def product(args, dist: Dist):
     return out
 
 
+# ---------------------------------------------------------------- batched leg
+def batched(args):
+    """64 independent 3D Euler cases (seeded blasts / oblique shock tubes,
+    grid edges round(32 * 4**u), u ~ U[0,1] per axis, random Roe / AUSM x
+    MUSCL / WENO5, SSP-RK3, FP32 flux, TEXTBOOK compat: the reference's WENO
+    goes to NaN on the strongest blasts) advanced together: one persistent
+    launch per scheme group and stage, one CUDA graph per step. Compared with
+    the same cases run one engine at a time (sum of their device times)."""
+    import numpy as np
+
+    from fvm3d import abi, cases, tuning
+    from fvm3d.solver import Solver
+
+    rng = np.random.default_rng(2024)
+    cs = []
+    for i in range(args.batch_cases):
+        n = tuple(int(round(32 * 4 ** u)) for u in rng.uniform(size=3))
+        recon = [abi.RECON_MUSCL, abi.RECON_WENO][int(rng.integers(2))]
+        flux = [abi.FLUX_ROE, abi.FLUX_AUSM][int(rng.integers(2))]
+        fam = cases.blast if rng.uniform() < 0.5 else cases.shock_tube
+        cs.append(fam(n, seed=int(rng.integers(1 << 30)), reconstruct=recon, flux_split=flux,
+                      limiter=abi.LIMITER_MINMOD, kappa=1.0 / 3.0, precision=abi.PREC_FP32_FLUX,
+                      compat=abi.COMPAT_TEXTBOOK))
+    cells = sum(c.ncells for c in cs)
+    steps = max(3, min(args.steps, 20))
+    s = Solver(cs[0].config())
+    s.remove_case(0)
+    for c in cs:
+        cid = s.add_case(c.config())
+        c.case_id = cid
+        c.apply(s, case_id=cid, states=False)
+    for c in cs:
+        for b, q in enumerate(c.states):
+            s.set_state(c.block_ids[b], q)
+    s.step(2)
+    ms = tuning.time_step(s, steps)
+    failed = sum(1 for c in cs if s.case_state(c.case_id)["status"] != 0)
+    groups = len({(c.cfg["reconstruct"], c.cfg["flux_split"]) for c in cs})
+    launches = tuning.launches_per_step(s)
+    s.close()
+    seq_ms = 0.0
+    for c in cs:
+        a = c.apply(Solver(c.config()))
+        a.step(1)
+        seq_ms += tuning.time_step(a, steps)
+        a.close()
+    return {"cases": len(cs), "cells": cells, "scheme_groups": groups, "steps": steps, "ms_per_step": ms,
+            "cases_nonfinite": failed,
+            "value": cells * 3 / (ms * 1e-3) / 1e9, "unit": UNIT, "kernel_launches_per_step": launches,
+            "one_at_a_time": {"ms_per_step": seq_ms, "value": cells * 3 / (seq_ms * 1e-3) / 1e9},
+            "dtype": "f32 recon/flux, f64 state"}
+
+
+# ---------------------------------------------------------------- serving leg
+def serve(args):
+    """Poisson stream of seeded 3D Euler requests (blast / shock tube, cubes
+    of 32^3..96^3 cells, 100..400 SSP-RK3 steps, random schemes, FP32 flux)
+    served with continuous batching in a 4 GB state budget, against the same
+    stream served one request at a time."""
+    from fvm3d import abi, serving
+
+    make = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(32, 96))
+    budget = int(4e9 / (5 * 8 * 3))
+    rate = 40.0
+    out = {}
+    st = serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=(100, 400))
+    srv = serving.Server(budget_cells=budget, chunk=16)
+    out["continuous_batching"] = srv.run(st)
+    srv.close()
+    st = serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=(100, 400))
+    out["one_at_a_time"] = serving.serve_one_at_a_time(st)
+    out["arrival_rate_per_s"] = rate
+    out["budget_bytes"] = budget * 5 * 8 * 3
+    out["workload"] = ("seeded blasts / oblique shock tubes, 32^3..96^3, 100..400 RK3 steps, Poisson arrivals; "
+                       "reduced from 32^3..192^3 / 200..2000 steps to keep the bench within minutes")
+    return out
+
+
 # ---------------------------------------------------------------- CPU oracle
 def cpu_oracle(n, steps, warmup, threads=None):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -340,6 +422,13 @@ def main():
     line.update({"value": res.pop("value"), "ms_per_step": res.pop("ms_per_step"),
                  "dtype": "f32 recon/flux, f64 state + RK + dt + norms"})
     line.update(res)
+    if dist.world == 1 and not args.no_batch:
+        line["batched"] = batched(args)
+    if dist.world == 1 and not args.no_serve:
+        sv = serve(args)
+        line["serving"] = sv
+        line["p50_s"] = sv["continuous_batching"]["p50_s"]
+        line["p99_s"] = sv["continuous_batching"]["p99_s"]
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         v, th, sec = cpu_oracle(args.n, 2, 0)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port",

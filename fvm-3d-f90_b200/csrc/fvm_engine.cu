@@ -528,7 +528,7 @@ int Engine::plan() {
     int64_t off = -1;
     if (alloc_range(b.padded, &off) != 0) {
       if (reserved_ > 0) return fail(FVM_ERR_NOMEM, "HBM budget exhausted: the reserved arena has no room");
-      int rc = grow_arena(need);
+      int rc = grow_arena(std::max(need, cap_ + cap_ / 2));
       if (rc) return rc;
       if (alloc_range(b.padded, &off) != 0) return fail(FVM_ERR_NOMEM, "arena allocation failed");
     }

@@ -117,6 +117,12 @@ __device__ __forceinline__ void to_stencil(const double q[5], R s[5], double gm1
   }
 }
 
+// TEXTBOOK compat only: a reconstructed face state with non-positive density
+// or pressure is replaced by the first-order state (the cell's own value).
+template <class R> __device__ __forceinline__ bool admissible(const Prim5<R>& p) {
+  return p.r > R(0) && p.p > R(0);
+}
+
 template <class R> __device__ __forceinline__ Prim5<R> mkprim(const R s[5]) {
   Prim5<R> p;
   p.r = s[0]; p.u = s[1]; p.v = s[2]; p.w = s[3]; p.p = s[4];
@@ -347,6 +353,11 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
             zWcur = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
           else
             zWcur = zWm_cur;
+          if (K.textbook && !(admissible(zWm_cur) && admissible(zWcur))) {
+            const Prim5<R> pc = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
+            if (!admissible(zWm_cur)) zWm_cur = pc;
+            if (!admissible(zWcur)) zWcur = pc;
+          }
         }
         if (do_xy) {
           for (int w = tid; w < C::NXN + C::NYN; w += NT) {
@@ -371,6 +382,8 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
 #pragma unroll
             for (int v = 0; v < 5; ++v) wm[v] = weno5<R, EX>(u[v][0], u[v][1], u[v][2], u[v][3], u[v][4], K.textbook);
             Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
+            if (K.textbook && !admissible(pm))
+              pm = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
             constexpr int NN = C::NXN + C::NYN;
             sN[0 * NN + w] = pm.r;
             sN[1 * NN + w] = pm.u;
@@ -382,6 +395,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
 #pragma unroll
               for (int v = 0; v < 5; ++v) wp[v] = weno5<R, EX>(u[v][4], u[v][3], u[v][2], u[v][1], u[v][0], 1);
               Prim5<R> pp = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
+              if (!admissible(pp)) pp = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
               sN[5 * NN + w] = pp.r;
               sN[6 * NN + w] = pp.u;
               sN[7 * NN + w] = pp.v;
@@ -410,6 +424,10 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
             }
             L = mkprim(l);
             Rr = mkprim(r);
+            if (K.textbook) {
+              if (!admissible(L)) L = mkprim(zw[1]);
+              if (!admissible(Rr)) Rr = mkprim(zw[2]);
+            }
           } else {
             L = mkprim(zw[1]);
             Rr = mkprim(zw[2]);
@@ -448,6 +466,16 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
               }
               L = mkprim(l);
               Rr = mkprim(r);
+              if (RECON == RECON_MUSCL_ && K.textbook && !(admissible(L) && admissible(Rr))) {
+                R c0[5], c1[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                  c0[v] = sP[v * PLANE + base - 1];
+                  c1[v] = sP[v * PLANE + base];
+                }
+                if (!admissible(L)) L = mkprim(c0);
+                if (!admissible(Rr)) Rr = mkprim(c1);
+              }
             }
             face_flux<FLUX, 0, R, EX>(L, Rr, K, F);
           } else {
@@ -477,6 +505,16 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
               }
               L = mkprim(l);
               Rr = mkprim(r);
+              if (RECON == RECON_MUSCL_ && K.textbook && !(admissible(L) && admissible(Rr))) {
+                R c0[5], c1[5];
+#pragma unroll
+                for (int v = 0; v < 5; ++v) {
+                  c0[v] = sP[v * PLANE + base - PW];
+                  c1[v] = sP[v * PLANE + base];
+                }
+                if (!admissible(L)) L = mkprim(c0);
+                if (!admissible(Rr)) Rr = mkprim(c1);
+              }
             }
             face_flux<FLUX, 1, R, EX>(L, Rr, K, F);
           }

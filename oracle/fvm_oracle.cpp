@@ -591,6 +591,14 @@ void inviscid_dir(orc_ctx* c, Block& b, int dir) {
           }
         }
       }
+      // TEXTBOOK only (EXTENSION): a reconstructed state with non-positive
+      // density or pressure falls back to the first-order state of its cell
+      if (cfg.compat == FVM_COMPAT_TEXTBOOK && cfg.reconstruct != FVM_RECON_SIMPLE) {
+        for (int64_t f = 1; f <= nface; ++f) {
+          if (!(pm[f - 1].rho > 0.0 && pm[f - 1].press > 0.0)) pm[f - 1] = b.p[g0 + (f + dghost - 1 - 1) * gs];
+          if (!(pp[f - 1].rho > 0.0 && pp[f - 1].press > 0.0)) pp[f - 1] = b.p[g0 + (f + dghost - 1) * gs];
+        }
+      }
       // flux (scheme_FDS_Roe / scheme_FVS_VanLeer / scheme_AUSM)
       std::vector<double> flux(nface * 5);
       for (int64_t f = 0; f < nface; ++f) {

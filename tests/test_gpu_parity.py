@@ -138,3 +138,23 @@ def test_primitive_download():
     c = cases.riemann2d(n=20, seed=0, dt=1e-3)
     g, o, _, _ = run_both(c, 2)
     assert np.array_equal(g.get_primitive(0), o.get_primitive(0))
+
+
+def test_textbook_positivity_fallback_exact():
+    # a strong blast where the reference's WENO + AUSM produces NaN (see the
+    # oracle test); TEXTBOOK compat falls back to first-order face states
+    c = cases.blast((20, 20, 20), seed=0, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM,
+                    compat=abi.COMPAT_TEXTBOOK)
+    g, o, (tg, rag, _), (to, rao, _, _) = run_both(c, 3)
+    assert np.array_equal(g.get_state(0), o.get_state(0))
+    assert np.isfinite(rag).all()
+
+
+def test_reference_blast_reports_nonfinite():
+    from fvm3d.solver import FvmError
+
+    c = cases.blast((20, 20, 20), seed=0, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM)
+    g = c.apply(Solver(c.config()))
+    with pytest.raises(FvmError) as e:
+        g.step(2)
+    assert e.value.code == 4 and "NaN" in e.value.msg

@@ -227,3 +227,17 @@ def test_vortex_converges_to_exact():
         ex = cases.vortex_exact(c, t)[0]
         errs.append(np.abs(o.get_state(0)[0] - ex[0]).mean())
     assert errs[1] < 0.5 * errs[0]
+
+
+def test_reference_weno_blast_nan_and_textbook_fallback():
+    # the reference reconstructs conservative variables without a positivity
+    # limit: on a strong blast its face states go negative and the residual
+    # becomes NaN (its converged() then stops with "Error: ABSRES NaN");
+    # TEXTBOOK compat falls back to first-order states there
+    c = cases.blast((20, 20, 20), seed=0, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM)
+    _, (t, ra, rr, dt) = _run(c, 2)
+    assert np.isnan(ra[5])
+    c = cases.blast((20, 20, 20), seed=0, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM,
+                    compat=abi.COMPAT_TEXTBOOK)
+    o, (t, ra, rr, dt) = _run(c, 3)
+    assert np.isfinite(ra).all() and np.isfinite(o.get_state(0)).all()
