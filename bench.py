@@ -66,9 +66,14 @@ class Dist:
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
         if self.world > 1:
-            # one process per GPU; the library uses the first visible device
-            if "CUDA_VISIBLE_DEVICES" not in os.environ:
+            # one process per GPU: the library uses the first visible device,
+            # so each rank keeps only its own entry of the visible list
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            if vis is None:
                 os.environ["CUDA_VISIBLE_DEVICES"] = str(self.local)
+            elif vis.strip():
+                devs = [d for d in vis.split(",") if d.strip()]
+                os.environ["CUDA_VISIBLE_DEVICES"] = devs[self.local % len(devs)].strip()
             import datetime
 
             import torch.distributed as dist
@@ -350,6 +355,31 @@ def batched(args):
             "dtype": "f32 recon/flux, f64 state"}
 
 
+# ---------------------------------------------------------------- Navier-Stokes leg
+def tgv(args):
+    """Compressible Taylor-Green vortex, 128^3, Ma 0.1, Re 1600, Pr 0.71,
+    MUSCL / Van Albada + Roe + central viscous flux, SSP-RK3, CFL 0.5: FP64
+    plain and FP32 flux, with the kinetic-energy difference after the steps."""
+    from fvm3d import abi, cases, tuning
+    from fvm3d.solver import Solver
+
+    c = cases.taylor_green(N=128)
+    steps = max(3, min(args.steps, 20))
+    out = {"cells": c.ncells, "steps": steps}
+    dV = c.meta["dx"] ** 3
+    ke = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_flux", abi.PREC_FP32_FLUX)):
+        s = c.apply(Solver(c.config(precision=prec)))
+        s.step(1)
+        ms = tuning.time_step(s, steps)
+        ke[name] = cases.kinetic_energy(s.get_state(0), dV)
+        out[name] = {"ms_per_step": ms, "value": c.ncells * 3 / (ms * 1e-3) / 1e9}
+        s.close()
+    out["ke_rel_diff_fp32_vs_fp64"] = abs(ke["fp32_flux"] - ke["fp64"]) / ke["fp64"]
+    out["unit"] = UNIT
+    return out
+
+
 # ---------------------------------------------------------------- serving leg
 def serve(args):
     """Poisson stream of seeded 3D Euler requests (blast / shock tube, cubes
@@ -424,6 +454,8 @@ def main():
     line.update(res)
     if dist.world == 1 and not args.no_batch:
         line["batched"] = batched(args)
+    if dist.world == 1 and not args.no_batch:
+        line["navier_stokes_tgv"] = tgv(args)
     if dist.world == 1 and not args.no_serve:
         sv = serve(args)
         line["serving"] = sv

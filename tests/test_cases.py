@@ -57,3 +57,28 @@ def test_riemann_seed_ranges():
     c = cases.riemann2d(n=32, seed=5)
     for rho, u, v, w, p in c.meta["quadrants"]:
         assert 0.5 <= rho <= 1.5 and 0.3 <= p <= 1.5 and -0.5 <= u <= 0.5 and -0.5 <= v <= 0.5
+
+
+def test_integer_factorization_prefers_small_cuts():
+    from fvm3d import partition
+
+    assert partition.integer_factorize((128, 128, 128), 8) == (2, 2, 2)
+    assert partition.integer_factorize((256, 32, 32), 4) == (4, 1, 1)
+    with __import__("pytest").raises(ValueError):
+        partition.integer_factorize((4, 4, 4), 8, min_cells=3)
+
+
+def test_partitioned_case_equals_single_block():
+    import oracle as orc
+    from fvm3d import abi, partition
+
+    c1 = cases.isentropic_vortex(N=24, layout="single", rk_stages=3, reconstruct=abi.RECON_MUSCL,
+                                 limiter=abi.LIMITER_MINMOD, flux_split=abi.FLUX_ROE)
+    c6 = partition.partition_case(c1, 6, periodic=(True, True, True))
+    assert len(c6.blocks) == 6
+    o1 = c1.apply(orc.Oracle(c1.config()))
+    o6 = c6.apply(orc.Oracle(c6.config()))
+    o1.step(2)
+    o6.step(2)
+    q6 = cases.assemble(c6, [o6.get_state(b) for b in range(6)])
+    assert np.array_equal(q6, o1.get_state(0))

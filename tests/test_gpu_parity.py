@@ -158,3 +158,23 @@ def test_reference_blast_reports_nonfinite():
     with pytest.raises(FvmError) as e:
         g.step(2)
     assert e.value.code == 4 and "NaN" in e.value.msg
+
+
+def test_tgv_kinetic_energy_history():
+    # Navier-Stokes Taylor-Green vortex: the kinetic-energy history of the
+    # exact FP64 path equals the oracle's bit for bit; the FP32 flux form
+    # tracks it to 1e-6 relative
+    c = cases.taylor_green(N=24)
+    dV = c.meta["dx"] ** 3
+    g = c.apply(Solver(c.config()))
+    f = c.apply(Solver(c.config(precision=abi.PREC_FP32_FLUX)))
+    o = c.apply(orc.Oracle(c.config()))
+    for _ in range(4):
+        g.step(1)
+        f.step(1)
+        o.step(1)
+        kg = cases.kinetic_energy(g.get_state(0), dV)
+        ko = cases.kinetic_energy(o.get_state(0), dV)
+        kf = cases.kinetic_energy(f.get_state(0), dV)
+        assert kg == ko
+        assert abs(kf - ko) <= 1e-6 * ko
