@@ -28,12 +28,12 @@ struct StageKernelInfo {
 };
 
 // Tile shapes compiled for every scheme (index -> TX x TY, minimum resident
-// CTAs per SM the register allocation is capped for; 0 = 2 for the FP32 flux
-// form and 1 for FP64).
-constexpr int kNumTiles = 3;
-constexpr int kTileTX[kNumTiles] = {32, 16, 32};
-constexpr int kTileTY[kNumTiles] = {8, 16, 8};
-constexpr int kTileMinB[kNumTiles] = {0, 0, 2};
+// CTAs per SM the register allocation is capped for; 0 = 16 warps per SM for
+// the FP32 flux form and 8 for FP64, i.e. 2 / 1 CTAs of 256 threads).
+constexpr int kNumTiles = 4;
+constexpr int kTileTX[kNumTiles] = {32, 16, 32, 16};
+constexpr int kTileTY[kNumTiles] = {8, 16, 8, 8};
+constexpr int kTileMinB[kNumTiles] = {0, 0, 2, 0};
 
 // prec: 0 exact FP64, 1 FP64, 2 FP32 flux; dim 2|3; recon 200..202;
 // flux 300|301|303; tb: textbook WENO (mirrored right state); tile 0..kNumTiles-1.

@@ -20,6 +20,35 @@ namespace fvm {
 
 namespace {
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Split nz planes into chunks of at most L planes, all of nearly equal length
+// (lengths differ by at most one plane).
+inline void equal_chunks(int64_t nz, int64_t L, std::vector<int64_t>& z0s) {
+  z0s.clear();
+  const int64_t nc = std::max<int64_t>(1, (nz + L - 1) / L);
+  const int64_t base = nz / nc, extra = nz % nc;
+  int64_t z = 0;
+  for (int64_t c = 0; c < nc; ++c) {
+    z0s.push_back(z);
+    z += base + (c < extra ? 1 : 0);
+  }
+  z0s.push_back(nz);
+}
+
+// Makespan of the persistent work queue for tasks of the given costs on
+// `slots` CTAs: tasks are taken longest first, each by the CTA that frees
+// first (what the atomic task counter does when costs are uniform per plane).
+double queue_makespan(std::vector<double>& cost, int slots) {
+  std::sort(cost.begin(), cost.end(), std::greater<double>());
+  std::vector<double> heap(std::max(1, slots), 0.0);  // min-heap of finish times
+  auto cmp = std::greater<double>();
+  for (double c : cost) {
+    std::pop_heap(heap.begin(), heap.end(), cmp);
+    heap.back() += c;
+    std::push_heap(heap.begin(), heap.end(), cmp);
+  }
+  return *std::max_element(heap.begin(), heap.end());
+}
 inline int stage_roles(int S, int m, int* rin, int* rout) {
   // RK3: A->B, (A,B)->C, (A,C)->A. RK4: A->B, B->C, C->B, B->A (q0 = A).
   static const int r3[3][2] = {{ROLE_A, ROLE_B}, {ROLE_B, ROLE_C}, {ROLE_C, ROLE_A}};
@@ -615,28 +644,53 @@ int Engine::plan() {
       if (hc.group != (int)g) continue;
       // z chunk from the case's own size only, so a case is tiled the same
       // whether it runs alone or batched with others
-      int64_t cols_planes = 0;
-      for (int bi : hc.blocks) {
-        const HBlock& b = blocks[bi];
-        cols_planes += ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty) * b.n[2];
-      }
       int64_t L = hc.zchunk;
       if (G.dim == 3 && L <= 0) {
-        L = (cols_planes + 3 * (int64_t)G.grid - 1) / (3 * (int64_t)G.grid);
-        L = std::max<int64_t>(8, round_up(L, 4));
+        if (hc.auto_key == std::make_pair(G.tile, G.grid)) {
+          L = hc.auto_zchunk;
+        } else {
+          // Pick the chunk length whose simulated queue makespan is lowest.
+          // A task of c planes costs c plane-times plus the warm-up of its z
+          // window (WENO: 2 planes of z-only work, MUSCL 1) and its set-up.
+          const double ovh = G.recon == FVM_RECON_WENO ? 1.0 : (G.recon == FVM_RECON_MUSCL ? 0.65 : 0.35);
+          double best = 0.0;
+          std::vector<double> cost;
+          std::vector<int64_t> z0s;
+          for (int64_t cand = 64; cand >= 4; cand -= (cand > 16 ? 4 : 2)) {
+            cost.clear();
+            for (int bi : hc.blocks) {
+              const HBlock& b = blocks[bi];
+              const int64_t ncol = ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty);
+              equal_chunks(b.n[2], cand, z0s);
+              for (size_t c = 0; c + 1 < z0s.size(); ++c)
+                for (int64_t q = 0; q < ncol; ++q) cost.push_back((double)(z0s[c + 1] - z0s[c]) + ovh);
+            }
+            const double m = queue_makespan(cost, G.grid);
+            if (L <= 0 || m < best * 0.995) {
+              best = m;
+              L = cand;
+            }
+          }
+          hc.auto_key = std::make_pair(G.tile, G.grid);
+          hc.auto_zchunk = L;
+        }
       }
+      std::vector<int64_t> z0s;
       for (int bi : hc.blocks) {
         const HBlock& b = blocks[bi];
-        const int64_t Lb = (G.dim == 3) ? std::min<int64_t>(L, b.n[2]) : b.n[2];
-        for (int64_t z0 = 0; z0 < b.n[2]; z0 += Lb)
+        if (G.dim == 3)
+          equal_chunks(b.n[2], L, z0s);
+        else
+          z0s = {0, b.n[2]};
+        for (size_t c = 0; c + 1 < z0s.size(); ++c)
           for (int64_t y0 = 0; y0 < b.n[1]; y0 += G.k.ty)
             for (int64_t x0 = 0; x0 < b.n[0]; x0 += G.k.tx) {
               Task t;
               t.blk = bi;
               t.x0 = (int)x0;
               t.y0 = (int)y0;
-              t.z0 = (int)z0;
-              t.z1 = (int)std::min<int64_t>(z0 + Lb, b.n[2]);
+              t.z0 = (int)z0s[c];
+              t.z1 = (int)z0s[c + 1];
               t.slot = 0;
               gt.push_back(t);
             }

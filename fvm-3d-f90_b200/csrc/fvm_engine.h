@@ -57,7 +57,10 @@ struct HCase {
   bool fresh = true;    // device state (time, residual history) not initialised
   int group = -1;
   int tile = -1;        // forced tile (autotuner result), -1 = heuristic
-  int zchunk = 0;       // forced z chunk, 0 = heuristic
+  int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model
+  // cost-model choice cached per (tile, grid); depends on the case alone
+  std::pair<int, int> auto_key{-1, -1};
+  int64_t auto_zchunk = 0;
 };
 
 struct Group {

@@ -35,20 +35,33 @@ struct StageCfg {
   using R = typename PrecT<PREC>::R;
   static constexpr bool EX = PrecT<PREC>::ex;
   static constexpr int H = RECON == RECON_WENO_ ? 3 : (RECON == RECON_MUSCL_ ? 2 : 1);
-  static constexpr int NT = TX * TY;
+  static constexpr int NC = TX * TY;  // column threads: one z column (a cell of each plane) each
+  // threads of the CTA: NC rounded up to one warp per scheduler; a tile
+  // smaller than its launch leaves whole warps that take only x / y node and
+  // face items
+  static constexpr int NT = (NC + 127) / 128 * 128;
   static constexpr int PW = TX + 2 * H, PH = TY + 2 * H;
   static constexpr int NODEV = RECON == RECON_WENO_ ? (TB ? 10 : 5) : 0;
   static constexpr int NXN = (TX + 2) * TY, NYN = TX * (TY + 2);
   static constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);
   static constexpr int NW = 2 * H * (TX + TY);             // halo cells of a plane
-  static constexpr int NPL = (DIM == 2 ? NT : 0) + NW;     // plane cells loaded from HBM
+  static constexpr int NPL = (DIM == 2 ? NC : 0) + NW;     // plane cells loaded from HBM
   static constexpr int NPS = (NPL + NT - 1) / NT;          // per-thread load slots
   static constexpr int WIN = H + 2;                        // z window: planes k-1 .. k+H
   static constexpr int WZ = RECON == RECON_WENO_ ? 2 : 1;  // warm-up planes before z0
   // R arrays first, then the FP64 staging of the cell's q0 / q_in / acc
   static constexpr size_t r_elems = (size_t)(5 * PH * PW + NODEV * (NXN + NYN) + 5 * (NXF + NYF));
   static constexpr size_t stage_off = (sizeof(R) * r_elems + 15) / 16 * 16;
-  static constexpr size_t smem_bytes = stage_off + sizeof(double) * 3 * 5 * NT;
+  // The next plane's loads are prefetched asynchronously into shared memory
+  // in the FP32 flux form; the FP64 forms, whose shared arrays are twice as
+  // large, prefetch into registers so that two CTAs still fit on an SM.
+  static constexpr bool PSM = sizeof(R) == 4;
+  // FP64 arrays: [2][5][NC] RK operands (q0, then q_in or acc), [6][NT] the
+  // column's residual sums and wave-speed maximum and, with PSM, the prefetch
+  // of the next plane's loaded cells [5][NPL] and, in 3D, of the z window's
+  // next plane [5][NC], both as loaded (conservative FP64)
+  static constexpr int NPRE = PSM ? 5 * NPL + (DIM == 3 ? 5 * NC : 0) : 0;
+  static constexpr size_t smem_bytes = stage_off + sizeof(double) * (2 * 5 * NC + 6 * NT + NPRE);
 };
 
 // ---------------------------------------------------------------- helpers
@@ -140,11 +153,15 @@ __device__ __forceinline__ double wavespeed(const double q[5], double gamma, dou
   return s;
 }
 
-// Deterministic CTA reduction of 5 sums and 1 max into partials[slot].
+// Deterministic CTA reduction of the column accumulators sS[6][NT] (5 sums,
+// 1 max) into partials[slot].
 template <int NT>
-__device__ __forceinline__ void cta_reduce_store(double ss[5], double wm, double* red, double* dst) {
+__device__ __forceinline__ void cta_reduce_store(const double* sS, double* red, double* dst) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = NT / 32;
+  double ss[5], wm = sS[5 * NT + threadIdx.x];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) ss[v] = sS[v * NT + threadIdx.x];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -196,23 +213,29 @@ __device__ __forceinline__ void plane_cell(int w, int& xx, int& yy) {
 
 // ---------------------------------------------------------------- kernel
 template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, int MINB>
-__global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 2 : 1)))
+__global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::NT,
+                                  (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 512 : 256) / (TX * TY)))
     stage_kernel(const StageArgs a) {
   using C = StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>;
   using R = typename C::R;
   constexpr bool EX = C::EX;
-  constexpr int H = C::H, NT = C::NT, PW = C::PW, PH = C::PH;
+  constexpr int H = C::H, NT = C::NT, NC = C::NC, PW = C::PW, PH = C::PH;
   constexpr int PLANE = PH * PW;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);   // [5][PH][PW]   plane k + halo
   R* sN = sP + 5 * PLANE;                   // [NODEV][NXN+NYN] x/y WENO nodes
   R* sF = sN + C::NODEV * (C::NXN + C::NYN);  // [5][NXF+NYF]  x/y face fluxes
-  double* sQ = reinterpret_cast<double*>(smem_raw + C::stage_off);  // [3][5][NT] q0, q_in, acc
+  double* sQ = reinterpret_cast<double*>(smem_raw + C::stage_off);  // [2][5][NC] q0, q_in | acc
+  double* sS = sQ + 2 * 5 * NC;                                       // [6][NT] residual / wave speed
+  double* sX = sS + 6 * NT;                                           // [5][NPL] next plane's loads
+  double* sZ = sX + 5 * C::NPL;                                       // [5][NC] z window's next plane (3D)
   __shared__ double s_red[6 * (NT / 32)];
   __shared__ int s_task;
 
   const int tid = threadIdx.x;
+  // column threads own a z column; the others (whole warps) skip all z work
+  const bool colt = (NC == NT) || tid < NC;
   const int tx = tid % TX, ty = tid / TX;
 
   for (;;) {
@@ -258,11 +281,12 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
     const bool need_acc = (rk_stages == 4 && a.m >= 2);
 
     const int nxt = min(TX, G.n0 - T.x0), nyt = min(TY, G.n1 - T.y0);
-    const bool act = tx < nxt && ty < nyt;
+    const bool act = colt && tx < nxt && ty < nyt;
     const int gx = T.x0 + tx, gy = T.y0 + ty;
 
-    double ss[5] = {0, 0, 0, 0, 0};
-    double wmax = 0.0;
+    if (a.last)
+#pragma unroll
+      for (int v = 0; v < 6; ++v) sS[v * NT + tid] = 0.0;
 
     // loop-invariant (x, y) parts of this thread's plane loads
     int lxy[C::NPS], lsp[C::NPS];
@@ -286,6 +310,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
     R zFprev[5] = {0, 0, 0, 0, 0};
     const int kstart = (DIM == 3) ? T.z0 - C::WZ : T.z0;
     if constexpr (DIM == 3) {
+      if (colt)
 #pragma unroll
       for (int s = 0; s < C::WIN; ++s) {
         double q[5];
@@ -313,16 +338,38 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       const bool more = (k + 1 < T.z1);
       const bool more_xy = more && (k + 1 >= T.z0);  // plane k+1 lies in [z0, z1)
 
-      // ---- prefetch the next plane's halo (and z window plane) into registers
-      double pre[C::NPS][5];
+      // ---- prefetch the next plane's loaded cells (and the z window's next
+      // plane): into shared memory with PSM (each thread later reads only its
+      // own copies), else into registers.
+      double pre[C::PSM ? 1 : C::NPS][5];
       double zpre[5];
+      if (more_xy) {
 #pragma unroll
-      for (int sidx = 0; sidx < C::NPS; ++sidx) {
-        if (more_xy && lsp[sidx] >= 0) ld5(qin, (int64_t)lxy[sidx] + (int64_t)(k + 1) * G.sz, vs, pre[sidx]);
+        for (int sidx = 0; sidx < C::NPS; ++sidx) {
+          if (lsp[sidx] >= 0) {
+            const double* src = qin + (int64_t)lxy[sidx] + (int64_t)(k + 1) * G.sz;
+            if constexpr (C::PSM) {
+              const int w = tid + sidx * NT;
+#pragma unroll
+              for (int v = 0; v < 5; ++v) __pipeline_memcpy_async(sX + v * C::NPL + w, src + v * vs, sizeof(double));
+            } else {
+              ld5(src, 0, vs, pre[sidx]);
+            }
+          }
+        }
       }
       if constexpr (DIM == 3) {
-        if (more) ld5(qin, (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz, vs, zpre);
+        if (more && colt) {
+          const double* src = qin + (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz;
+          if constexpr (C::PSM) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) __pipeline_memcpy_async(sZ + v * NC + tid, src + v * vs, sizeof(double));
+          } else {
+            ld5(src, 0, vs, zpre);
+          }
+        }
       }
+      if constexpr (C::PSM) __pipeline_commit();
 
       // ---- the cell's RK operands of plane k, copied asynchronously into
       // shared memory; phase C waits for this thread's own copies only.
@@ -330,9 +377,9 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       if (do_xy && act) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          __pipeline_memcpy_async(sQ + (0 * 5 + v) * NT + tid, q0p + off_k + v * vs, sizeof(double));
-          if (need_um) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NT + tid, qin + off_k + v * vs, sizeof(double));
-          if (need_acc) __pipeline_memcpy_async(sQ + (2 * 5 + v) * NT + tid, accp + off_k + v * vs, sizeof(double));
+          __pipeline_memcpy_async(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs, sizeof(double));
+          if (need_um) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NC + tid, qin + off_k + v * vs, sizeof(double));
+          if (need_acc) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NC + tid, accp + off_k + v * vs, sizeof(double));
         }
         __pipeline_commit();
       }
@@ -340,7 +387,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       // ---- phase A: WENO nodes --------------------------------------------
       Prim5<R> zWcur, zWm_cur;
       if constexpr (RECON == RECON_WENO_) {
-        if constexpr (DIM == 3) {
+        if (DIM == 3 && colt) {
           // node of plane k+1 from planes k-1 .. k+3 (window slots 0..4)
           R wm[5], wp[5];
 #pragma unroll
@@ -410,7 +457,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       // ---- phase B: fluxes ---------------------------------------------------
       R zF[5] = {0, 0, 0, 0, 0};
       if constexpr (DIM == 3) {
-        if (k >= T.z0 - 1) {
+        if (colt && k >= T.z0 - 1) {
           Prim5<R> L, Rr;
           if constexpr (RECON == RECON_WENO_) {
             L = zWprev;
@@ -564,9 +611,9 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
         __pipeline_wait_prior(0);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          u0[v] = sQ[(0 * 5 + v) * NT + tid];
-          um[v] = need_um ? sQ[(1 * 5 + v) * NT + tid] : 0.0;
-          ac[v] = need_acc ? sQ[(2 * 5 + v) * NT + tid] : 0.0;
+          u0[v] = sQ[(0 * 5 + v) * NC + tid];
+          um[v] = need_um ? sQ[(1 * 5 + v) * NC + tid] : 0.0;
+          ac[v] = need_acc ? sQ[(1 * 5 + v) * NC + tid] : 0.0;
         }
         double h = dtg;
         if (ts_set == 2) h = cfl / wavespeed(u0, gammad, gm1d, drv, idim);
@@ -609,8 +656,8 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
         for (int v = 0; v < 5; ++v) qout[off + v * vs] = out[v];
         if (a.last) {
 #pragma unroll
-          for (int v = 0; v < 5; ++v) ss[v] += rhs[v] * rhs[v];
-          if (ts_set != 0) wmax = fmax(wmax, wavespeed(out, gammad, gm1d, drv, idim));
+          for (int v = 0; v < 5; ++v) sS[v * NT + tid] += rhs[v] * rhs[v];
+          if (ts_set != 0) sS[5 * NT + tid] = fmax(sS[5 * NT + tid], wavespeed(out, gammad, gm1d, drv, idim));
           if (rhs_out) {
             const int64_t nc = (int64_t)G.n0 * G.n1 * G.n2;
             const int64_t r0 = gx + (int64_t)G.n0 * (gy + (int64_t)G.n1 * k);
@@ -621,7 +668,8 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       }
 
       // ---- carry, window shift and shared-memory refill ----------------------
-      if constexpr (DIM == 3) {
+      if constexpr (C::PSM) __pipeline_wait_prior(0);
+      if (DIM == 3 && colt) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) zFprev[v] = zF[v];
         if constexpr (RECON == RECON_WENO_) zWprev = zWm_cur;
@@ -629,7 +677,13 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
         for (int s = 0; s + 1 < C::WIN; ++s)
 #pragma unroll
           for (int v = 0; v < 5; ++v) zw[s][v] = zw[s + 1][v];
-        if (more) to_stencil<RECON, R, EX>(zpre, zw[C::WIN - 1], gm1d, K.gm1);
+        if (more) {
+          if constexpr (C::PSM) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) zpre[v] = sZ[v * NC + tid];
+          }
+          to_stencil<RECON, R, EX>(zpre, zw[C::WIN - 1], gm1d, K.gm1);
+        }
         if (more_xy) {
           // centre of plane k+1 is window slot 1 after the shift
 #pragma unroll
@@ -640,8 +694,17 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
 #pragma unroll
         for (int sidx = 0; sidx < C::NPS; ++sidx) {
           if (lsp[sidx] >= 0) {
+            double q[5];
+            if constexpr (C::PSM) {
+              const int w = tid + sidx * NT;
+#pragma unroll
+              for (int v = 0; v < 5; ++v) q[v] = sX[v * C::NPL + w];
+            } else {
+#pragma unroll
+              for (int v = 0; v < 5; ++v) q[v] = pre[sidx][v];
+            }
             R s[5];
-            to_stencil<RECON, R, EX>(pre[sidx], s, gm1d, K.gm1);
+            to_stencil<RECON, R, EX>(q, s, gm1d, K.gm1);
 #pragma unroll
             for (int v = 0; v < 5; ++v) sP[v * PLANE + lsp[sidx]] = s[v];
           }
@@ -650,7 +713,7 @@ __global__ void __launch_bounds__(TX* TY, (MINB > 0 ? MINB : (PREC == PREC_FP32 
       __syncthreads();
     }
 
-    if (a.last) cta_reduce_store<NT>(ss, wmax, s_red, a.partials + (int64_t)T.slot * kPartStride);
+    if (a.last) cta_reduce_store<NT>(sS, s_red, a.partials + (int64_t)T.slot * kPartStride);
   }
 }
 

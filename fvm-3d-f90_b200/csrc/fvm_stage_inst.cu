@@ -23,7 +23,7 @@ static bool fill(StageKernelInfo* out) {
   using Cfg = StageCfg<FVM_RECON, FLUX, FVM_PREC, TB, DIM, TX, TY>;
   out->fn = reinterpret_cast<const void*>(&stage_kernel<FVM_RECON, FLUX, FVM_PREC, TB, DIM, TX, TY, MINB>);
   out->smem = Cfg::smem_bytes;
-  out->threads = TX * TY;
+  out->threads = Cfg::NT;
   out->tx = TX;
   out->ty = TY;
   return true;
@@ -35,6 +35,7 @@ static bool by_tile(int tile, StageKernelInfo* out) {
     case 0: return fill<FLUX, TB, DIM, kTileTX[0], kTileTY[0], kTileMinB[0]>(out);
     case 1: return fill<FLUX, TB, DIM, kTileTX[1], kTileTY[1], kTileMinB[1]>(out);
     case 2: return fill<FLUX, TB, DIM, kTileTX[2], kTileTY[2], kTileMinB[2]>(out);
+    case 3: return fill<FLUX, TB, DIM, kTileTX[3], kTileTY[3], kTileMinB[3]>(out);
     default: return false;
   }
 }

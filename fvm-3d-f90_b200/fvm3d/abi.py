@@ -141,11 +141,13 @@ _lib = None
 
 
 def load_library(path: str | None = None) -> ctypes.CDLL:
-    """Load libfvm3d.so and declare its prototypes. Raises if it is absent."""
+    """Load libfvm3d.so and declare its prototypes. Raises if it is absent.
+    The environment variable FVM3D_LIB, when set, names another build of the
+    library to load instead of the in-tree one."""
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("FVM3D_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise OSError(
             f"libfvm3d.so not found at {p}; build it with "

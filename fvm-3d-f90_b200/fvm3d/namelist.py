@@ -188,12 +188,15 @@ def parse_case(text: str) -> CaseSpec:
 def initial_state(spec: CaseSpec):
     """The initial condition the reference hard-codes for every case file
     (the 2D Riemann quadrants of class_flow_field.f90:207-243) on the grid
-    the file describes."""
+    the file describes). Its four regions cover [0,1]^2 only; a larger grid
+    would keep zero density outside them, so it is rejected."""
     import numpy as np
 
     from . import cases
 
     ni, nj, nk = spec.nvert
+    if spec.dr[0] * (ni - 1) > 1.0 + 1e-12 or spec.dr[1] * (nj - 1) > 1.0 + 1e-12:
+        raise NamelistError("the reference initial condition covers the unit square only (geoSize <= 1)")
     x = spec.dr[0] * np.arange(ni)
     y = spec.dr[1] * np.arange(nj)
     X, Y = np.meshgrid(x, y, indexing="xy")

@@ -17,7 +17,7 @@ CASE = """
 &Geometry
   type      = "uniform"
   geoType   = "square"
-  geoSize   = 2.0
+  geoSize   = 1.0
   gridType  = "nodal-centered"
   gridSize  = 33, &
               33
@@ -61,7 +61,7 @@ def test_parse_maps_keys_to_config():
     assert c.flux_split == abi.FLUX_AUSM and c.entropy_fix == 0.1
     assert c.time_scheme == abi.TIME_RUNGE_KUTTA and c.timestep_set == abi.DT_FIXED and c.dt == 1e-3
     assert spec.nvert == (33, 33, 2)
-    assert spec.dr == pytest.approx((2.0 / 32, 2.0 / 32, 1.0))
+    assert spec.dr == pytest.approx((1.0 / 32, 1.0 / 32, 1.0))
     assert spec.total_time == 0.005 and spec.absolute_residual == 1e-12 and spec.relative_residual == 1e-9
 
 
@@ -87,6 +87,13 @@ def test_format_error():
 def test_unknown_scheme_is_rejected():
     with pytest.raises(NamelistError, match="Invalid flux split scheme"):
         parse_case(CASE.replace('"AUSM"', '"Godunov"'))
+
+
+def test_initial_state_outside_unit_square_is_rejected():
+    from fvm3d.namelist import initial_state
+
+    with pytest.raises(NamelistError, match="unit square"):
+        initial_state(parse_case(CASE.replace("geoSize   = 1.0", "geoSize   = 2.0")))
 
 
 def test_extension_group():
