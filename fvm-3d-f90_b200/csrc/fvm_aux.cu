@@ -205,64 +205,148 @@ __device__ __forceinline__ double vcomp(const VPrim& p, int m) {
   return m == 0 ? p.u : (m == 1 ? p.v : (m == 2 ? p.w : p.th));
 }
 
-// Viscous flux through the face between cells cL and cL + e_dir.
-__device__ void visc_face(const DevBlock& B, const DevCase& C, const double* q, int dir, int x, int y, int z,
-                          double G[5]) {
-  int e[3] = {0, 0, 0};
-  e[dir] = 1;
-  const double gm1 = C.gm1;
-  const VPrim L = vprim(q, vcell(B, x, y, z), B.vs, gm1);
-  const VPrim R = vprim(q, vcell(B, x + e[0], y + e[1], z + e[2]), B.vs, gm1);
+// Viscous flux G[1..4] (G[0] = 0) through a face normal to `dir` between
+// cells L and R. tg[d] holds, for each tangential axis d != dir, the cells
+// L + e_d, L - e_d, R + e_d, R - e_d; the tangential gradient is the mean of
+// the two central differences.
+__device__ __forceinline__ void visc_flux(const VPrim& L, const VPrim& R, const VPrim (*tg)[4], int dir,
+                                          const double dr[3], double mu, double kq, int idim, double G[5]) {
   double grad[4][3];
   for (int m = 0; m < 4; ++m)
     for (int d = 0; d < 3; ++d) grad[m][d] = 0.0;
-  for (int m = 0; m < 4; ++m) grad[m][dir] = (vcomp(R, m) - vcomp(L, m)) / B.dr[dir];
-  for (int d = 0; d < C.idim; ++d) {
+  for (int m = 0; m < 4; ++m) grad[m][dir] = (vcomp(R, m) - vcomp(L, m)) / dr[dir];
+  for (int d = 0; d < idim; ++d) {
     if (d == dir) continue;
-    int t[3] = {0, 0, 0};
-    t[d] = 1;
-    const VPrim lp = vprim(q, vcell(B, x + t[0], y + t[1], z + t[2]), B.vs, gm1);
-    const VPrim lm = vprim(q, vcell(B, x - t[0], y - t[1], z - t[2]), B.vs, gm1);
-    const VPrim rp = vprim(q, vcell(B, x + e[0] + t[0], y + e[1] + t[1], z + e[2] + t[2]), B.vs, gm1);
-    const VPrim rm = vprim(q, vcell(B, x + e[0] - t[0], y + e[1] - t[1], z + e[2] - t[2]), B.vs, gm1);
+    const VPrim& lp = tg[d][0];
+    const VPrim& lm = tg[d][1];
+    const VPrim& rp = tg[d][2];
+    const VPrim& rm = tg[d][3];
     for (int m = 0; m < 4; ++m)
-      grad[m][d] = ((vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m))) / (4.0 * B.dr[d]);
+      grad[m][d] = ((vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m))) / (4.0 * dr[d]);
   }
   const double div = grad[0][0] + grad[1][1] + grad[2][2];
   const double uf[3] = {0.5 * (L.u + R.u), 0.5 * (L.v + R.v), 0.5 * (L.w + R.w)};
   double tau[3];
   for (int m = 0; m < 3; ++m) {
-    tau[m] = C.mu * (grad[m][dir] + grad[dir][m]);
-    if (m == dir) tau[m] = tau[m] - 2.0 / 3.0 * C.mu * div;
+    tau[m] = mu * (grad[m][dir] + grad[dir][m]);
+    if (m == dir) tau[m] = tau[m] - 2.0 / 3.0 * mu * div;
   }
   G[0] = 0.0;
   G[1] = tau[0];
   G[2] = tau[1];
   G[3] = tau[2];
-  G[4] = uf[0] * tau[0] + uf[1] * tau[1] + uf[2] * tau[2] + C.kq * grad[3][dir];
+  G[4] = uf[0] * tau[0] + uf[1] * tau[1] + uf[2] * tau[2] + kq * grad[3][dir];
 }
 
-__global__ void visc_kernel(const DevBlock* blocks, const DevCase* cases, int role) {
-  const DevBlock B = blocks[blockIdx.y];
-  const DevCase C = cases[B.case_id];
-  if (!B.visc) return;
+// Tiled viscous kernel: one CTA per task (a TX x TY column tile over a z
+// range). The cell primitives (u, v, w, p/rho) of planes k-1, k, k+1 with a
+// one-cell halo sit in a shared-memory ring; each x / y face flux of plane k
+// is computed once into shared memory, each z face once per column (the lower
+// one carried in registers). V = (dGx + dGy) + dGz as in the per-cell form.
+template <int TX, int TY, int IDIM>
+__global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* blocks, const DevCase* cases,
+                                                          const Task* tasks, int role) {
+  constexpr int NT = TX * TY, PX = TX + 2, PY = TY + 2, PL = PX * PY;
+  constexpr int NR = IDIM == 3 ? 3 : 1;
+  constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1), NF = NXF + NYF;
+  __shared__ VPrim sp[NR][PL];
+  __shared__ double sg[4][NF];
+
+  const Task T = tasks[blockIdx.x];
+  const DevBlock& B = blocks[T.blk];
+  const DevCase& C = cases[B.case_id];
   const double* q = B.q[role];
-  const int64_t nc = (int64_t)B.n[0] * B.n[1] * B.n[2];
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(c % B.n[0]);
-    const int64_t r = c / B.n[0];
-    const int j = (int)(r % B.n[1]), k = (int)(r / B.n[1]);
-    double V[5] = {0, 0, 0, 0, 0};
-    for (int dir = 0; dir < C.idim; ++dir) {
-      int e[3] = {0, 0, 0};
-      e[dir] = 1;
-      double Gl[5], Gr[5];
-      visc_face(B, C, q, dir, i - e[0], j - e[1], k - e[2], Gl);
-      visc_face(B, C, q, dir, i, j, k, Gr);
-      for (int v = 0; v < 5; ++v) V[v] = V[v] + (Gr[v] - Gl[v]) / B.dr[dir];
+  const int64_t vs = B.vs;
+  const double gm1 = C.gm1, mu = C.mu, kq = C.kq;
+  const double dr[3] = {B.dr[0], B.dr[1], B.dr[2]};
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const bool act = (T.x0 + tx < B.n[0]) && (T.y0 + ty < B.n[1]);
+  auto slot = [](int z) { return IDIM == 3 ? ((z % 3) + 3) % 3 : 0; };
+  // cell primitives of plane z, halo included; positions stay within the
+  // first ghost layer (partial tiles clamp onto it)
+  auto fill = [&](int z) {
+    VPrim* dst = sp[slot(z)];
+    for (int w = tid; w < PL; w += NT) {
+      const int x = min(max(T.x0 + w % PX - 1, -1), B.n[0]);
+      const int y = min(max(T.y0 + w / PX - 1, -1), B.n[1]);
+      dst[w] = vprim(q, vcell(B, x, y, z), vs, gm1);
     }
-    const int64_t o = i + (int64_t)j * B.sy + (int64_t)k * B.sz;
-    for (int v = 0; v < 5; ++v) B.visc[o + v * B.vs] = V[v];
+  };
+  auto P = [&](int z, int x, int y) -> const VPrim& { return sp[slot(z)][(y + 1) * PX + (x + 1)]; };
+  // z face between planes z and z+1 of this thread's column
+  auto zface = [&](int z, double G[5]) {
+    VPrim tg[3][4];
+    tg[0][0] = P(z, tx + 1, ty);
+    tg[0][1] = P(z, tx - 1, ty);
+    tg[0][2] = P(z + 1, tx + 1, ty);
+    tg[0][3] = P(z + 1, tx - 1, ty);
+    tg[1][0] = P(z, tx, ty + 1);
+    tg[1][1] = P(z, tx, ty - 1);
+    tg[1][2] = P(z + 1, tx, ty + 1);
+    tg[1][3] = P(z + 1, tx, ty - 1);
+    visc_flux(P(z, tx, ty), P(z + 1, tx, ty), tg, 2, dr, mu, kq, 3, G);
+  };
+
+  double Gzl[5] = {0, 0, 0, 0, 0}, Gzr[5] = {0, 0, 0, 0, 0};
+  if (IDIM == 3) {
+    fill(T.z0 - 1);
+    fill(T.z0);
+  }
+  for (int k = T.z0; k < T.z1; ++k) {
+    fill(IDIM == 3 ? k + 1 : k);
+    __syncthreads();
+    for (int w = tid; w < NF; w += NT) {
+      VPrim tg[3][4];
+      double G[5];
+      if (w < NXF) {
+        const int f = w % (TX + 1), row = w / (TX + 1);  // face between cells f-1 and f
+        tg[1][0] = P(k, f - 1, row + 1);
+        tg[1][1] = P(k, f - 1, row - 1);
+        tg[1][2] = P(k, f, row + 1);
+        tg[1][3] = P(k, f, row - 1);
+        if (IDIM == 3) {
+          tg[2][0] = P(k + 1, f - 1, row);
+          tg[2][1] = P(k - 1, f - 1, row);
+          tg[2][2] = P(k + 1, f, row);
+          tg[2][3] = P(k - 1, f, row);
+        }
+        visc_flux(P(k, f - 1, row), P(k, f, row), tg, 0, dr, mu, kq, IDIM, G);
+      } else {
+        const int w2 = w - NXF, col = w2 % TX, f = w2 / TX;  // face between rows f-1 and f
+        tg[0][0] = P(k, col + 1, f - 1);
+        tg[0][1] = P(k, col - 1, f - 1);
+        tg[0][2] = P(k, col + 1, f);
+        tg[0][3] = P(k, col - 1, f);
+        if (IDIM == 3) {
+          tg[2][0] = P(k + 1, col, f - 1);
+          tg[2][1] = P(k - 1, col, f - 1);
+          tg[2][2] = P(k + 1, col, f);
+          tg[2][3] = P(k - 1, col, f);
+        }
+        visc_flux(P(k, col, f - 1), P(k, col, f), tg, 1, dr, mu, kq, IDIM, G);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) sg[v][w] = G[v + 1];
+    }
+    if (IDIM == 3) {
+      if (k == T.z0) zface(k - 1, Gzl);
+      zface(k, Gzr);
+    }
+    __syncthreads();
+    if (act) {
+      const int fxl = ty * (TX + 1) + tx, fyl = NXF + ty * TX + tx;
+      double V[5] = {0, 0, 0, 0, 0};
+      for (int v = 1; v < 5; ++v) {
+        V[v] = V[v] + (sg[v - 1][fxl + 1] - sg[v - 1][fxl]) / dr[0];
+        V[v] = V[v] + (sg[v - 1][fyl + TX] - sg[v - 1][fyl]) / dr[1];
+        if (IDIM == 3) V[v] = V[v] + (Gzr[v] - Gzl[v]) / dr[2];
+      }
+      V[0] = 0.0 + (0.0 - 0.0) / dr[0];
+      const int64_t o = (T.x0 + tx) + (int64_t)(T.y0 + ty) * B.sy + (int64_t)k * B.sz;
+      for (int v = 0; v < 5; ++v) B.visc[o + v * vs] = V[v];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) Gzl[v] = Gzr[v];
   }
 }
 
@@ -311,10 +395,13 @@ cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_visc(const DevBlock* blocks, int nblocks, const DevCase* cases, int role, cudaStream_t s) {
-  if (nblocks == 0) return cudaSuccess;
-  dim3 g(128, nblocks);
-  visc_kernel<<<g, 128, 0, s>>>(blocks, cases, role);
+cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
+                        int role, cudaStream_t s) {
+  if (ntasks == 0) return cudaSuccess;
+  if (idim == 3)
+    visc_tile_kernel<kViscTX, kViscTY, 3><<<ntasks, kViscTX * kViscTY, 0, s>>>(blocks, cases, tasks, role);
+  else
+    visc_tile_kernel<kViscTX, kViscTY, 2><<<ntasks, kViscTX * kViscTY, 0, s>>>(blocks, cases, tasks, role);
   return cudaGetLastError();
 }
 

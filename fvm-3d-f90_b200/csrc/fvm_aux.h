@@ -17,7 +17,12 @@ cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* c
                            unsigned long long* case_max, int role, cudaStream_t s);
 cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                             int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s);
-cudaError_t launch_visc(const DevBlock* blocks, int nblocks, const DevCase* cases, int role, cudaStream_t s);
+// Viscous contribution of the Navier-Stokes blocks: one CTA per task of the
+// viscous task list (kViscTX x kViscTY column tiles over z ranges), all of
+// dimension idim.
+constexpr int kViscTX = 16, kViscTY = 8, kViscZ = 16;
+cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
+                        int role, cudaStream_t s);
 
 // One compiled instantiation of the fused stage kernel.
 struct StageKernelInfo {

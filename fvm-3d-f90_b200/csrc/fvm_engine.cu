@@ -714,6 +714,36 @@ int Engine::plan() {
   }
   ntasks_total = (int64_t)tasks.size();
 
+  // -- viscous task list: Navier-Stokes blocks in column tiles over equal z
+  // chunks, 3D blocks first, then 2D
+  vtask_off_ = (int)tasks.size();
+  for (int dim : {3, 2}) {
+    const int before = (int)tasks.size();
+    std::vector<int64_t> z0s;
+    for (int bi : live_blocks) {
+      const HBlock& b = blocks[bi];
+      const fvm_config& c = cases[b.case_id].cfg;
+      if (c.equation != FVM_EQ_NAVIER_STOKES || c.idimension != dim) continue;
+      if (dim == 3)
+        equal_chunks(b.n[2], kViscZ, z0s);
+      else
+        z0s = {0, b.n[2]};
+      for (size_t ch = 0; ch + 1 < z0s.size(); ++ch)
+        for (int64_t y0 = 0; y0 < b.n[1]; y0 += kViscTY)
+          for (int64_t x0 = 0; x0 < b.n[0]; x0 += kViscTX) {
+            Task t;
+            t.blk = bi;
+            t.x0 = (int)x0;
+            t.y0 = (int)y0;
+            t.z0 = (int)z0s[ch];
+            t.z1 = (int)z0s[ch + 1];
+            t.slot = 0;
+            tasks.push_back(t);
+          }
+    }
+    (dim == 3 ? nvtask3_ : nvtask2_) = (int)tasks.size() - before;
+  }
+
   // -- ghost gather pairs (slab element offsets)
   std::vector<int64_t> pairs;
   auto add_pair = [&](int bi, const int64_t x[3]) -> int {
@@ -868,9 +898,6 @@ int Engine::plan() {
 // the finalize. With `evs`, an event is recorded after every launch and the
 // kind of each launch (1 stage, 2 gather, 3 viscous, 4 finalize) returned.
 int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
-  bool any_ns = false;
-  for (auto& c : cases)
-    if (!c.dead) any_ns |= c.cfg.equation == FVM_EQ_NAVIER_STOKES;
   const int S = max_stages_;
   // groups run as parallel branches of the captured graph (fork / join on
   // side streams); the profiled path launches them in sequence to time each
@@ -891,8 +918,12 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
   for (int m = 1; m <= S; ++m) {
     int rin, rout;
     stage_roles(S, m, &rin, &rout);
-    if (any_ns) {
-      CK(launch_visc(d_blocks_, (int)blocks.size(), d_cases_, rin, stream));
+    if (nvtask3_ > 0) {
+      CK(launch_visc(d_blocks_, d_cases_, d_tasks_ + vtask_off_, nvtask3_, 3, rin, stream));
+      CK(mark(3));
+    }
+    if (nvtask2_ > 0) {
+      CK(launch_visc(d_blocks_, d_cases_, d_tasks_ + vtask_off_ + nvtask3_, nvtask2_, 2, rin, stream));
       CK(mark(3));
     }
     if (fork) CK(cudaEventRecord(fork_ev_[ev_i], stream));

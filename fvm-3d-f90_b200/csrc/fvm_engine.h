@@ -154,6 +154,7 @@ class Engine {
   int64_t* d_pairs_ = nullptr;
   int* d_counters_ = nullptr;
   int ncounters_ = 0;
+  int vtask_off_ = 0, nvtask3_ = 0, nvtask2_ = 0;  // viscous tasks in d_tasks_
   unsigned long long* d_casemax_ = nullptr;
   double* d_staging_ = nullptr;
   size_t staging_bytes_ = 0;

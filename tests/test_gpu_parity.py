@@ -112,6 +112,23 @@ def test_navier_stokes_tgv_exact():
     np.testing.assert_allclose(rag, rao, rtol=1e-12)
 
 
+def test_navier_stokes_blocks_exact():
+    # 8 uneven periodic blocks: connected faces and the layer-1 edge ghosts of
+    # the viscous stencil, partial viscous tiles
+    c = cases.isentropic_vortex(N=20, layout="blocks8", equation=abi.EQ_NAVIER_STOKES, mu=0.02, rk_stages=3,
+                                reconstruct=abi.RECON_MUSCL, limiter=abi.LIMITER_VANALBADA, flux_split=abi.FLUX_ROE)
+    g, o, _, _ = run_both(c, 3)
+    for b in range(8):
+        assert np.array_equal(g.get_state(b), o.get_state(b))
+
+
+def test_navier_stokes_2d_exact():
+    # 2D viscous path, transmissive regions, two independent k planes
+    c = cases.riemann2d(n=27, seed=3, nk=2, dt=1e-3, equation=abi.EQ_NAVIER_STOKES, mu=5e-3)
+    g, o, _, _ = run_both(c, 3)
+    assert np.array_equal(g.get_state(0), o.get_state(0))
+
+
 def test_fast_fp64_smooth_1e12():
     c = cases.isentropic_vortex(N=32, layout="blocks8")
     g, o, _, _ = run_both(c, 5, gpu_over=dict(precision=abi.PREC_FP64))
