@@ -112,46 +112,56 @@ __global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const uns
 // checks of converged (:180-188) and the next step's dt.
 __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                                 const double* partials, int* counters, int ncounters) {
-  __shared__ double red[6][256];
-  const int c = blockIdx.x, tid = threadIdx.x;
+  // one warp per block reduces its task partials (lanes stride the tasks,
+  // then a butterfly); thread 0 folds the blocks in order, as the reference
+  // accumulates them (class_iteration.f90:195-259)
+  constexpr int NW = 8;
+  __shared__ double red[NW][6];
+  const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const DevCase& C = cases[c];
   if (c == 0)
     for (int i = tid; i < ncounters; i += blockDim.x) counters[i] = 0;
   if (C.nblocks == 0) return;  // removed case
   double res[6] = {0, 0, 0, 0, 0, 0};
   double wmax = 0.0;
-  for (int bb = 0; bb < C.nblocks; ++bb) {
-    const DevBlock& B = blocks[case_blk[C.block0 + bb]];
-    double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
-    for (int t = tid; t < B.ntask; t += blockDim.x) {
-      const double* p = partials + (int64_t)(B.task0 + t) * kPartStride;
+  for (int b0 = 0; b0 < C.nblocks; b0 += NW) {
+    const int bb = b0 + warp;
+    if (warp < NW && bb < C.nblocks) {
+      const DevBlock& B = blocks[case_blk[C.block0 + bb]];
+      double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
+      for (int t = lane; t < B.ntask; t += 32) {
+        const double* p = partials + (int64_t)(B.task0 + t) * kPartStride;
 #pragma unroll
-      for (int v = 0; v < 5; ++v) s[v] += p[v];
-      m = fmax(m, p[5]);
+        for (int v = 0; v < 5; ++v) s[v] += p[v];
+        m = fmax(m, p[5]);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], o);
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) red[warp][v] = s[v];
+        red[warp][5] = m;
+      }
     }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) red[v][tid] = s[v];
-    red[5][tid] = m;
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if (tid < w) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) red[v][tid] += red[v][tid + w];
-        red[5][tid] = fmax(red[5][tid], red[5][tid + w]);
-      }
-      __syncthreads();
-    }
     if (tid == 0) {
-      const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
-      double res2[5], res2_t = 0.0;
-      for (int v = 0; v < 5; ++v) {
-        res2[v] = red[v][0] / npt;
-        res2_t = res2_t + res2[v];
+      for (int w = 0; w < NW && b0 + w < C.nblocks; ++w) {
+        const DevBlock& B = blocks[case_blk[C.block0 + b0 + w]];
+        const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
+        double res2[5], res2_t = 0.0;
+        for (int v = 0; v < 5; ++v) {
+          res2[v] = red[w][v] / npt;
+          res2_t = res2_t + res2[v];
+        }
+        res2_t = res2_t / 5.0;
+        for (int v = 0; v < 5; ++v) res[v] = sqrt(res[v] * res[v] + res2[v]);
+        res[5] = sqrt(res[5] * res[5] + res2_t);
+        wmax = fmax(wmax, red[w][5]);
       }
-      res2_t = res2_t / 5.0;
-      for (int v = 0; v < 5; ++v) res[v] = sqrt(res[v] * res[v] + res2[v]);
-      res[5] = sqrt(res[5] * res[5] + res2_t);
-      wmax = fmax(wmax, red[5][0]);
     }
     __syncthreads();
   }

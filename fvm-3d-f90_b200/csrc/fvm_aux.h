@@ -34,7 +34,7 @@ struct StageKernelInfo {
 
 // Tile shapes compiled for every scheme (index -> TX x TY, minimum resident
 // CTAs per SM the register allocation is capped for; 0 = 16 warps per SM for
-// the FP32 flux form and 8 for FP64, i.e. 2 / 1 CTAs of 256 threads).
+// the FP32 flux form, 12 for FP64 (rounded down to whole CTAs)).
 constexpr int kNumTiles = 4;
 constexpr int kTileTX[kNumTiles] = {32, 16, 32, 16};
 constexpr int kTileTY[kNumTiles] = {8, 16, 8, 8};

@@ -598,11 +598,13 @@ int Engine::plan() {
     const bool tb = c.reconstruct == FVM_RECON_WENO && c.compat == FVM_COMPAT_TEXTBOOK;
     int tile = hc.tile;
     if (tile < 0) {
-      // heuristic: 32 x 8 when the blocks are at least 32 wide, else 16 x 16;
-      // FP64 takes the register-capped 32 x 8 variant
+      // heuristic (the autotuner measures instead): 16 x 8 on 128 threads
+      // for the FP32 flux and FP64 forms; exact FP64, whose expression trees
+      // need more registers, takes the register-capped 32 x 8 variant when
+      // the blocks are at least 32 wide, else 16 x 16
       int64_t minx = 1 << 30;
       for (int b : hc.blocks) minx = std::min(minx, blocks[b].n[0]);
-      tile = (minx >= 32) ? (prec == FVM_PREC_FP32_FLUX ? 0 : 2) : 1;
+      tile = (prec != FVM_PREC_FP64_EXACT) ? 3 : (minx >= 32 ? 2 : 1);
     }
     int gi = -1;
     for (size_t g = 0; g < groups.size(); ++g) {

@@ -144,6 +144,73 @@ __device__ __forceinline__ R weno5(R u0, R u1, R u2, R u3, R u4, int textbook) {
   }
 }
 
+// Two WENO5 evaluations at once in packed FP32 (sm_100 f32x2 FMA / add /
+// multiply: one instruction per pair), for the FP32 flux form. Same formula as
+// weno5<float, false>; the pair shares `textbook`.
+__device__ __forceinline__ float2 f2_(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 weno5x2(float2 u0, float2 u1, float2 u2, float2 u3, float2 u4, int textbook) {
+  const float2 q0 = __ffma2_rn(f2_(1.0f / 3.0f), u0, __ffma2_rn(f2_(-7.0f / 6.0f), u1, __fmul2_rn(f2_(11.0f / 6.0f), u2)));
+  const float2 q1 = __ffma2_rn(f2_(-1.0f / 6.0f), u1, __ffma2_rn(f2_(5.0f / 6.0f), u2, __fmul2_rn(f2_(1.0f / 3.0f), u3)));
+  const float2 q2 = __ffma2_rn(f2_(1.0f / 3.0f), u2, __ffma2_rn(f2_(5.0f / 6.0f), u3, __fmul2_rn(f2_(-1.0f / 6.0f), u4)));
+  const float2 a0 = __ffma2_rn(f2_(-2.0f), u1, __fadd2_rn(u0, u2));
+  const float2 b0 = __ffma2_rn(f2_(-4.0f), u1, __ffma2_rn(f2_(3.0f), u2, u0));
+  const float2 a1 = __ffma2_rn(f2_(-2.0f), u2, __fadd2_rn(u1, u3));
+  const float2 b1 = textbook ? __ffma2_rn(f2_(-1.0f), u3, u1) : __fadd2_rn(u1, u3);
+  const float2 a2 = __ffma2_rn(f2_(-2.0f), u3, __fadd2_rn(u2, u4));
+  const float2 b2 = __ffma2_rn(f2_(3.0f), u2, __ffma2_rn(f2_(-4.0f), u3, u4));
+  // IS_k + eps = 13/12 a^2 + 1/4 b^2 + 1e-6
+  const float2 e0 = __ffma2_rn(__fmul2_rn(f2_(13.0f / 12.0f), a0), a0,
+                               __ffma2_rn(__fmul2_rn(f2_(0.25f), b0), b0, f2_(1.0e-6f)));
+  const float2 e1 = __ffma2_rn(__fmul2_rn(f2_(13.0f / 12.0f), a1), a1,
+                               __ffma2_rn(__fmul2_rn(f2_(0.25f), b1), b1, f2_(1.0e-6f)));
+  const float2 e2 = __ffma2_rn(__fmul2_rn(f2_(13.0f / 12.0f), a2), a2,
+                               __ffma2_rn(__fmul2_rn(f2_(0.25f), b2), b2, f2_(1.0e-6f)));
+  const float2 d0 = __fmul2_rn(e0, e0), d1 = __fmul2_rn(e1, e1), d2 = __fmul2_rn(e2, e2);
+  // weights c_k / d_k normalised: scale all by 1/c_0 (t0 = d1 d2, t1 = 6 d0 d2, t2 = 3 d0 d1)
+  const float2 t0 = __fmul2_rn(d1, d2);
+  const float2 t1 = __fmul2_rn(__fmul2_rn(f2_(6.0f), d0), d2);
+  const float2 t2 = __fmul2_rn(__fmul2_rn(f2_(3.0f), d0), d1);
+  const float2 num = __ffma2_rn(t0, q0, __ffma2_rn(t1, q1, __fmul2_rn(t2, q2)));
+  const float2 den = __fadd2_rn(t0, __fadd2_rn(t1, t2));
+  return __fmul2_rn(num, make_float2(rcp_(den.x), rcp_(den.y)));
+}
+
+// The WENO node values of one stencil u[var][0..4]: wm (left-biased, value
+// at the right face of u[.][2]) and, with TB, wp (mirrored, value at its left
+// face, always the textbook form). The FP32 flux form evaluates them in pairs.
+template <class R, bool EX, bool TB>
+__device__ __forceinline__ void weno5_node(const R (&u)[5][5], int textbook, R wm[5], R wp[5]) {
+  if constexpr (sizeof(R) == 4) {
+    if constexpr (TB) {
+      // TB implies TEXTBOOK compat, so both sides take the textbook form
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float2 r = weno5x2(make_float2(u[v][0], u[v][4]), make_float2(u[v][1], u[v][3]),
+                                 make_float2(u[v][2], u[v][2]), make_float2(u[v][3], u[v][1]),
+                                 make_float2(u[v][4], u[v][0]), 1);
+        wm[v] = r.x;
+        wp[v] = r.y;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; v += 2) {
+        const int w = v + 1 < 5 ? v + 1 : v;
+        const float2 r = weno5x2(make_float2(u[v][0], u[w][0]), make_float2(u[v][1], u[w][1]),
+                                 make_float2(u[v][2], u[w][2]), make_float2(u[v][3], u[w][3]),
+                                 make_float2(u[v][4], u[w][4]), textbook);
+        wm[v] = r.x;
+        if (v + 1 < 5) wm[v + 1] = r.y;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      wm[v] = weno5<R, EX>(u[v][0], u[v][1], u[v][2], u[v][3], u[v][4], textbook);
+      if (TB) wp[v] = weno5<R, EX>(u[v][4], u[v][3], u[v][2], u[v][1], u[v][0], 1);
+    }
+  }
+}
+
 // ------------------------------------------------------------ Roe
 // scheme_FDS_Roe.f90:25-177
 template <class R> __device__ __forceinline__ R entropy_fix_(R lam, R delta) {

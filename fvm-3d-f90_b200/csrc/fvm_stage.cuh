@@ -53,9 +53,10 @@ struct StageCfg {
   static constexpr size_t r_elems = (size_t)(5 * PH * PW + NODEV * (NXN + NYN) + 5 * (NXF + NYF));
   static constexpr size_t stage_off = (sizeof(R) * r_elems + 15) / 16 * 16;
   // The next plane's loads are prefetched asynchronously into shared memory
-  // in the FP32 flux form; the FP64 forms, whose shared arrays are twice as
-  // large, prefetch into registers so that two CTAs still fit on an SM.
-  static constexpr bool PSM = sizeof(R) == 4;
+  // in the FP32 flux form and in small FP64 tiles; the large FP64 tiles,
+  // whose shared arrays would then no longer fit twice on an SM, prefetch
+  // into registers.
+  static constexpr bool PSM = sizeof(R) == 4 || TX * TY <= 128;
   // FP64 arrays: [2][5][NC] RK operands (q0, then q_in or acc), [6][NT] the
   // column's residual sums and wave-speed maximum and, with PSM, the prefetch
   // of the next plane's loaded cells [5][NPL] and, in 3D, of the z window's
@@ -214,7 +215,7 @@ __device__ __forceinline__ void plane_cell(int w, int& xx, int& yy) {
 // ---------------------------------------------------------------- kernel
 template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, int MINB>
 __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::NT,
-                                  (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 512 : 256) / (TX * TY)))
+                                  (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 512 : 384) / (TX * TY)))
     stage_kernel(const StageArgs a) {
   using C = StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>;
   using R = typename C::R;
@@ -389,12 +390,12 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       if constexpr (RECON == RECON_WENO_) {
         if (DIM == 3 && colt) {
           // node of plane k+1 from planes k-1 .. k+3 (window slots 0..4)
-          R wm[5], wp[5];
+          R wm[5], wp[5], u[5][5];
 #pragma unroll
-          for (int v = 0; v < 5; ++v) {
-            wm[v] = weno5<R, EX>(zw[0][v], zw[1][v], zw[2][v], zw[3][v], zw[4][v], K.textbook);
-            if (TB) wp[v] = weno5<R, EX>(zw[4][v], zw[3][v], zw[2][v], zw[1][v], zw[0][v], 1);
-          }
+          for (int v = 0; v < 5; ++v)
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[v][s] = zw[s][v];
+          weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
           zWm_cur = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
           if (TB)
             zWcur = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
@@ -425,9 +426,8 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 #pragma unroll
                 for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s * PW];
             }
-            R wm[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) wm[v] = weno5<R, EX>(u[v][0], u[v][1], u[v][2], u[v][3], u[v][4], K.textbook);
+            R wm[5], wp[5];
+            weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
             Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
             if (K.textbook && !admissible(pm))
               pm = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
@@ -438,9 +438,6 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
             sN[3 * NN + w] = pm.w;
             sN[4 * NN + w] = pm.p;
             if (TB) {
-              R wp[5];
-#pragma unroll
-              for (int v = 0; v < 5; ++v) wp[v] = weno5<R, EX>(u[v][4], u[v][3], u[v][2], u[v][1], u[v][0], 1);
               Prim5<R> pp = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
               if (!admissible(pp)) pp = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
               sN[5 * NN + w] = pp.r;
