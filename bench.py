@@ -35,6 +35,7 @@ sys.path.insert(0, PKG)
 
 METRIC = "Gcell-stage/s FP64 plain vs FP32-batched at L1 err<=1e-6; served p50/p99 latency"
 UNIT = "Gcell-stage/s"
+STAGE_TRAFFIC_FP32 = 395.05e6  # bytes per stage launch, ncu dram__bytes_read.sum + dram__bytes_write.sum
 WORKLOAD = "isentropic vortex 3D Euler, periodic [-5,5]^3, 8 uneven blocks, 128^3 = 2,097,152 cells, WENO5 + AUSM, RK4, CFL 0.5"
 
 
@@ -232,7 +233,7 @@ def product(args, dist: Dist):
     # roofline of the dominant kernel (the fused stage): algorithmic bytes are
     # the FP64 state arrays each stage must read or write: RK4 stages touch
     # 3, 5, 5, 4 arrays of 5 x 8 B per cell = 680 B per cell-step.
-    def roof(prof):
+    def roof(prof, traffic=None):
         st = [ms for p in prof for k, ms in p if k == "stage"]
         per_step_ms = sum(st) / len(prof)
         alg = 680.0 * ncells
@@ -240,13 +241,17 @@ def product(args, dist: Dist):
         pk = peaks()
         share = per_step_ms / (sum(ms for p in prof for _, ms in p) / len(prof))
         return {"bound": "hbm", "achieved": round(ach, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": round(ach / pk["hbm_gbs"], 4), "traffic": None, "peak_src": pk["src"],
+                "frac": round(ach / pk["hbm_gbs"], 4), "traffic": traffic, "peak_src": pk["src"],
                 "stage_ms_per_step": round(per_step_ms, 4), "stage_share_of_step": round(share, 4),
-                "alg_bytes_per_cell_step": 680}
+                "alg_bytes_per_cell_step": 680, "alg_bytes_per_launch": round(170.0 * ncells)}
 
     out["value"] = gcs(ms32)
     out["ms_per_step"] = ms32
-    out["roofline"] = roof(prof32)
+    # DRAM bytes per stage launch (read + write, mean of the 4 launches of one
+    # step) from one ncu capture of the FP32 16x8 kernel on this workload;
+    # null for other workloads
+    traffic = STAGE_TRAFFIC_FP32 if ("fp32" in forms and args.n == 128) else None
+    out["roofline"] = roof(prof32, traffic)
     out["clocks"] = clocks
     out["gpu_launches"] = launches * args.steps
     if s64 is not None:
@@ -380,6 +385,33 @@ def tgv(args):
     return out
 
 
+# ---------------------------------------------------------------- 2D Riemann leg
+def riemann2d_leg(args):
+    """Four-quadrant 2D Riemann problem on 256 x 256 nodes of [0,1]^2, one
+    block, transmissive regions, MUSCL / minmod (kappa 1/3) + Roe (entropy fix
+    0.2), SSP-RK3, CFL 0.5: the reference's own kind of case at the size its
+    case files use, in the three precision forms. A 2D plane counts its cells
+    once."""
+    from fvm3d import abi, cases, tuning
+    from fvm3d.solver import Solver
+
+    c = cases.riemann2d(n=256, seed=11, reconstruct=abi.RECON_MUSCL, limiter=abi.LIMITER_MINMOD,
+                        kappa=1.0 / 3.0, flux_split=abi.FLUX_ROE, entropy_fix=0.2, rk_stages=3,
+                        timestep_set=abi.DT_CFL, cfl=0.5)
+    steps = max(20, args.steps * 10)
+    out = {"cells": c.ncells, "steps": steps}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_flux", abi.PREC_FP32_FLUX),
+                       ("fp64_exact", abi.PREC_FP64_EXACT)):
+        s = c.apply(Solver(c.config(precision=prec)))
+        s.step(3)
+        ms = tuning.time_step(s, steps)
+        out[name] = {"ms_per_step": ms, "value": c.ncells * 3 / (ms * 1e-3) / 1e9}
+        s.close()
+    out["unit"] = UNIT
+    out["note"] = "65,536 cells fill a fraction of the GPU: launch- and latency-bound (3 stage launches per step)"
+    return out
+
+
 # ---------------------------------------------------------------- serving leg
 def serve(args):
     """Poisson stream of seeded 3D Euler requests (blast / shock tube, cubes
@@ -456,6 +488,7 @@ def main():
         line["batched"] = batched(args)
     if dist.world == 1 and not args.no_batch:
         line["navier_stokes_tgv"] = tgv(args)
+        line["riemann2d_256"] = riemann2d_leg(args)
     if dist.world == 1 and not args.no_serve:
         sv = serve(args)
         line["serving"] = sv
@@ -466,6 +499,10 @@ def main():
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
                                 "sample": "2 RK4 steps of the full 8-block case on all host threads "
                                           f"({sec:.1f} s; C++ restatement of the reference path)"}
+        # the reference itself is serial: the same restatement on one thread
+        v1, _, sec1 = cpu_oracle(args.n, 1, 0, threads=1)
+        line["cpu_baseline_1thread"] = {"value": v1, "unit": UNIT, "cores": 1, "kind": "port",
+                                        "sample": f"1 RK4 step of the full 8-block case on one thread ({sec1:.1f} s)"}
     if dist.rank == 0:
         print(json.dumps(line))
     dist.close()

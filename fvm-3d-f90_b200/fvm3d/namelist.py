@@ -22,7 +22,7 @@ from __future__ import annotations
 
 from dataclasses import dataclass, field
 
-from . import abi
+from . import abi, output
 
 # the keys ClassInput%read_casefile asks for, per group (class_input.f90:109-177)
 GROUP_KEYS = {
@@ -112,6 +112,8 @@ class CaseSpec:
     absolute_residual: float
     relative_residual: float
     output_time: float
+    output_vars: tuple = ()
+    solnfile: str = ""
 
 
 DIMENSION = {"2D": 2, "3D": 3}
@@ -132,6 +134,7 @@ def parse_case(text: str) -> CaseSpec:
         nml.check()
         groups[g] = vals
     gen, geo, inv, ts = groups["General"], groups["Geometry"], groups["Inviscid_Flux"], groups["Time_Stepping"]
+    out = groups["Output"]
     ext = groups.get("B200", {})
 
     idim = DIMENSION.get(gen["dimension"])
@@ -182,7 +185,8 @@ def parse_case(text: str) -> CaseSpec:
                     total_time=_num(ts["total_time"], 0.0),
                     absolute_residual=_num(ts["absolute_residual"], 0.0),
                     relative_residual=_num(ts["relative_residual"], 0.0),
-                    output_time=_num(ts["output_time"], 0.0))
+                    output_time=_num(ts["output_time"], 0.0),
+                    output_vars=tuple(output.output_variables(out)), solnfile=out["solnfile"])
 
 
 def initial_state(spec: CaseSpec):
@@ -207,15 +211,37 @@ def initial_state(spec: CaseSpec):
     return np.broadcast_to(q[:, None], (5, nk, nj, ni)).copy()
 
 
-def run_case(text: str, solver_cls=None):
+def run_case(text: str, solver_cls=None, output_prefix: str | None = None):
     """Run a reference case file end to end: parse, build the block, upload
-    the reference IC, step until ClassIteration%converged fires."""
+    the reference IC, step until ClassIteration%converged fires. With
+    `output_prefix`, the flow field is written at t = 0 and whenever the time
+    hits the next multiple of output_time to 1e-9, as write_flowfield_sub
+    does (class_output.f90:204-237): once a time is missed, no later output
+    follows, as in the reference."""
     from .solver import Solver
 
     spec = parse_case(text)
     s = (solver_cls or Solver)(spec.config)
     s.add_block(spec.nvert, spec.dr)
     s.set_state(0, initial_state(spec))
-    steps, reason = s.run(total_time=spec.total_time, absolute_residual=spec.absolute_residual,
-                          relative_residual=spec.relative_residual)
+    stop = dict(absolute_residual=spec.absolute_residual, relative_residual=spec.relative_residual)
+    if output_prefix is None or not spec.output_vars:
+        steps, reason = s.run(total_time=spec.total_time, **stop)
+        return s, spec, steps, reason
+    w = output.SolutionWriter(output_prefix, spec.output_vars, spec.dr)
+    w.snapshot(s, 0.0, [0])
+    time_out, steps = spec.output_time, 0
+    while True:
+        chunked = spec.output_time > 0 and time_out < spec.total_time - 1e-10
+        n, reason = s.run(total_time=time_out if chunked else spec.total_time, **stop)
+        steps += n
+        t = s.time()[0]
+        if spec.output_time > 0 and abs(t - time_out) <= 1e-9:
+            w.snapshot(s, t, [0])
+            time_out += spec.output_time
+        elif chunked:
+            time_out = float("inf")   # missed: the reference writes nothing more
+        if not (chunked and reason == abi.STOP_MAX_TIME):
+            break
+    w.close()
     return s, spec, steps, reason
