@@ -463,11 +463,10 @@ int Engine::ensure_planned() {
   return plan();
 }
 
-int Engine::plan() {
-  if (gexec_) cudaGraphExecDestroy(gexec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  gexec_ = nullptr;
-  graph_ = nullptr;
+// Layout of the live blocks in the arena: region coverage checks, padded
+// boxes, arena ranges for new blocks (cleared once). Enough for state
+// uploads and downloads; plan() adds the work lists and the step graph.
+int Engine::layout() {
   std::vector<int> live_cases, live_blocks;
   for (size_t c = 0; c < cases.size(); ++c)
     if (!cases[c].dead) live_cases.push_back((int)c);
@@ -585,6 +584,25 @@ int Engine::plan() {
     staging_bytes_ = sizeof(double) * 5 * max_cells;
     CK(cudaMalloc(&d_staging_, staging_bytes_));
   }
+  laid_out_ = true;
+  return FVM_OK;
+}
+
+int Engine::plan() {
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  gexec_ = nullptr;
+  graph_ = nullptr;
+  if (!laid_out_) {
+    int rc = layout();
+    if (rc) return rc;
+  }
+  std::vector<int> live_cases, live_blocks;
+  for (size_t c = 0; c < cases.size(); ++c)
+    if (!cases[c].dead) live_cases.push_back((int)c);
+  for (size_t b = 0; b < blocks.size(); ++b)
+    if (!blocks[b].dead) live_blocks.push_back((int)b);
+  max_stages_ = cases[live_cases[0]].cfg.rk_stages;
 
   // -- groups (one per distinct kernel) and tasks
   groups.clear();
@@ -1043,12 +1061,14 @@ int Engine::prepare() {
 int Engine::set_state(int blk, const double* q) {
   if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!q) return fail(FVM_ERR_INVALID, "null state");
-  int rc = ensure_planned();
-  if (rc) return rc;
+  if (!laid_out_) {
+    int rc = layout();
+    if (rc) return rc;
+  }
   const HBlock& b = blocks[blk];
   const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
   CK(cudaMemcpyAsync(d_staging_, q, bytes, cudaMemcpyHostToDevice, stream));
-  CK(launch_unpack(h_dblocks_[blk].q[ROLE_A], cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
+  CK(launch_unpack(role_[ROLE_A] + b.slab_off + b.org, cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
                    d_staging_, stream));
   CK(cudaStreamSynchronize(stream));
   prepared_ = false;
@@ -1058,14 +1078,14 @@ int Engine::set_state(int blk, const double* q) {
 int Engine::get_state(int blk, double* q, int prim) {
   if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!q) return fail(FVM_ERR_INVALID, "null output");
-  if (!planned_) {
+  if (!laid_out_) {
     if (cap_ == 0) return fail(FVM_ERR_STATE, "no state uploaded yet");
-    int rc = plan();
+    int rc = layout();
     if (rc) return rc;
   }
   const HBlock& b = blocks[blk];
   const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
-  CK(launch_pack(h_dblocks_[blk].q[ROLE_A], cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
+  CK(launch_pack(role_[ROLE_A] + b.slab_off + b.org, cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
                  d_staging_, prim, cases[b.case_id].cfg.gamma - 1.0, stream));
   CK(cudaMemcpyAsync(q, d_staging_, bytes, cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
@@ -1101,7 +1121,10 @@ int Engine::step(int nsteps) {
 
 int Engine::read_case_state(int case_id, DevCaseState* out) {
   if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
-  if (!planned_) return fail(FVM_ERR_STATE, "no state uploaded yet");
+  // a case's device state exists from the first plan that saw it and
+  // survives later re-plans
+  if (!d_state_ || case_id >= state_cap_ || cases[case_id].fresh)
+    return fail(FVM_ERR_STATE, "no state uploaded yet");
   CK(cudaMemcpyAsync(out, d_state_ + case_id, sizeof(DevCaseState), cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
   return FVM_OK;

@@ -122,6 +122,7 @@ class Engine {
   int live_block(int blk) const { return blk >= 0 && blk < (int)blocks.size() && !blocks[blk].dead; }
 
  private:
+  int layout();
   int plan();
   int build_graph();
   int enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch);
@@ -129,6 +130,7 @@ class Engine {
   void invalidate() {  // topology changed: re-plan before the next use
     planned_ = false;
     prepared_ = false;
+    laid_out_ = false;
   }
   int alloc_range(int64_t size, int64_t* off);
   void free_range(int64_t off, int64_t size);
@@ -136,6 +138,7 @@ class Engine {
   int resolve(int blk, int64_t x[3], int* out_blk) const;
 
   bool planned_ = false;
+  bool laid_out_ = false;
   bool prepared_ = false;
   int nroles_ = 3;
   int max_stages_ = 3;

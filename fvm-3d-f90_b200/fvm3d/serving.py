@@ -84,7 +84,15 @@ def mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(32, 96)):
 class Server:
     """Continuous-batching server over one engine with a fixed state arena."""
 
-    def __init__(self, budget_cells: int, rk_stages: int = 3, chunk: int = 16):
+    def __init__(self, budget_cells: int, rk_stages: int = 3, chunk: int = 8, max_active_cells: int | None = 1 << 20):
+        """budget_cells: the state arena (HBM budget). max_active_cells: stop
+        admitting once the running set holds this many cells (None = no cap;
+        one request is always admitted into an empty set). Past the point
+        where the running set keeps the GPU busy, admitting more only shares
+        it among more requests, which lengthens every running request's
+        latency: on a B200, a cap of 2^20 cells measured p50 0.22 s against
+        0.45 s uncapped on the bench's 40 requests/s stream, at 4 % lower
+        throughput."""
         # the context's own first case is only a placeholder for the engine
         self.s = Solver(abi.make_config(rk_stages=rk_stages))
         self.s.remove_case(0)
@@ -92,6 +100,7 @@ class Server:
         self.budget = budget_cells
         self.free = budget_cells
         self.chunk = chunk
+        self.max_active_cells = max_active_cells
         self.active: list[Request] = []
         self.steps_run = 0
 
@@ -103,7 +112,11 @@ class Server:
         return sum(abi.block_cells(idim, n) for n, _ in c.blocks)
 
     def fits(self, r: Request) -> bool:
-        return r.cells <= self.free
+        if r.cells > self.free:
+            return False
+        if self.max_active_cells is not None and self.active:
+            return sum(a.cells for a in self.active) + r.cells <= self.max_active_cells
+        return True
 
     def admit(self, r: Request, now: float) -> bool:
         """Place the request's blocks in the arena and upload its state; on a

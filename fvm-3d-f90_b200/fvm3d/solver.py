@@ -124,9 +124,14 @@ class Solver:
                 "status": status.value}
 
     # -- state
+    def _shape(self, blk: int):
+        if not (0 <= blk < len(self.shapes)) or self.shapes[blk] is None:
+            raise FvmError(1, "bad block id")  # FVM_ERR_INVALID, as the ABI reports it
+        return self.shapes[blk]
+
     def set_state(self, blk: int, q: np.ndarray):
         """q: (5, nk, nj, ni) C-order, i.e. Fortran (ni,nj,nk,5)."""
-        ni, nj, nk = self.shapes[blk]
+        ni, nj, nk = self._shape(blk)
         a = np.ascontiguousarray(q, dtype=np.float64).reshape(5, nk, nj, ni)
         self._chk(self.lib.fvm_set_state(self.h, blk, _dp(a)))
 
@@ -138,7 +143,7 @@ class Solver:
         self._chk(self.lib.fvm_get_state(self.h, blk, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double))))
 
     def _get(self, fn, blk):
-        ni, nj, nk = self.shapes[blk]
+        ni, nj, nk = self._shape(blk)
         out = np.empty((5, nk, nj, ni), dtype=np.float64)
         self._chk(fn(self.h, blk, _dp(out)))
         return out

@@ -49,7 +49,9 @@ enum fvm_status {
   FVM_ERR_UNSUPPORTED = 8, /* id known to the reference but not implemented there either */
   FVM_ERR_BUSY = 9,        /* serving: no slot or memory free right now     */
   FVM_ERR_NOT_FOUND = 10,  /* serving: unknown request id                   */
-  FVM_ERR_NEGATIVE = 11    /* non-positive density or pressure in the state  */
+  FVM_ERR_NEGATIVE = 11    /* reserved: uploads are not validated (as in the
+                            * reference); a non-positive state surfaces as
+                            * FVM_ERR_NONFINITE at the next step             */
 };
 
 /* ---- scheme ids: the namelist strings map to these integers exactly as in

@@ -100,3 +100,23 @@ def test_server_results_same_alone_and_in_the_mix():
         ref = alone(r.case, r.nsteps)
         for got, want in zip(r.result, ref):
             assert np.array_equal(got, want), f"request {r.rid}"
+
+
+def test_server_admission_cap():
+    make = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(12, 24))
+    stream = serving.poisson_stream(8, rate=1000.0, seed=4, make_case=make, steps=(3, 12))
+    cells = [sum(abi.block_cells(3, n) for n, _ in r.case.blocks) for r in stream]
+    cap = 2 * max(cells)
+    seen = []
+
+    class Probe(serving.Server):
+        def admit(self, r, now):
+            ok = super().admit(r, now)
+            seen.append(sum(a.cells for a in self.active))
+            return ok
+
+    srv = Probe(budget_cells=10 * max(cells), chunk=2, max_active_cells=cap)
+    stats = srv.run(stream, realtime=False)
+    srv.close()
+    assert stats["requests"] == 8 and stats["failed"] == 0
+    assert max(seen) <= cap

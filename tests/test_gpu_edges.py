@@ -1,0 +1,91 @@
+"""Edge cases of the GPU path against the oracle: degenerate and ragged
+block shapes, the smallest periodic box, tiles that do not divide the block,
+and the error paths of the C ABI."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from fvm3d import abi, cases, tuning
+from fvm3d.solver import FvmError, Solver
+
+pytestmark = pytest.mark.gpu
+
+
+def both(case, steps, **over):
+    g = case.apply(Solver(case.config(**over)))
+    o = case.apply(orc.Oracle(case.config(**over)))
+    g.step(steps)
+    o.step(steps)
+    return g, o
+
+
+@pytest.mark.parametrize("n", [(1, 1, 1), (2, 3, 1), (7, 1, 5), (1, 9, 4), (5, 3, 2)])
+@pytest.mark.parametrize("recon,flux", [(abi.RECON_WENO, abi.FLUX_AUSM), (abi.RECON_MUSCL, abi.FLUX_ROE)])
+def test_degenerate_blocks_exact(n, recon, flux):
+    c = cases.shock_tube(n, seed=5, reconstruct=recon, flux_split=flux, limiter=abi.LIMITER_VANLEER,
+                         compat=abi.COMPAT_TEXTBOOK, rk_stages=3, timestep_set=abi.DT_FIXED, dt=1e-3)
+    g, o = both(c, 3)
+    assert np.array_equal(g.get_state(0), o.get_state(0))
+
+
+def test_smallest_periodic_box_exact():
+    # 3 cells per axis: every ghost layer of the 3-deep halo wraps onto the
+    # block itself
+    c = cases.isentropic_vortex(N=3, layout="single")
+    g, o = both(c, 2)
+    assert np.array_equal(g.get_state(0), o.get_state(0))
+
+
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
+def test_ragged_block_every_tile_exact(tile):
+    c = cases.shock_tube((37, 19, 11), seed=2, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_ROE,
+                         compat=abi.COMPAT_REFERENCE, rk_stages=4, timestep_set=abi.DT_CFL, cfl=0.4)
+    o = c.apply(orc.Oracle(c.config()))
+    o.step(3)
+    for prec in (abi.PREC_FP64_EXACT,):
+        g = Solver(c.config(precision=prec))
+        c.apply(g, states=False)
+        tuning.set_tuning(g, 0, tile, 0)
+        g.set_state(0, c.states[0])
+        g.step(3)
+        assert np.array_equal(g.get_state(0), o.get_state(0))
+
+
+def test_ragged_block_fp32_l1():
+    c = cases.shock_tube((37, 19, 11), seed=2, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM,
+                         compat=abi.COMPAT_TEXTBOOK, rk_stages=3, timestep_set=abi.DT_FIXED, dt=5e-4)
+    o = c.apply(orc.Oracle(c.config()))
+    o.step(5)
+    for tile in range(4):
+        g = Solver(c.config(precision=abi.PREC_FP32_FLUX))
+        c.apply(g, states=False)
+        tuning.set_tuning(g, 0, tile, 0)
+        g.set_state(0, c.states[0])
+        g.step(5)
+        err = np.abs(g.get_state(0)[0] - o.get_state(0)[0]).mean()
+        assert err <= 1e-6, (tile, err)
+
+
+def test_error_paths():
+    c = cases.shock_tube((8, 8, 8), seed=0, reconstruct=abi.RECON_MUSCL, flux_split=abi.FLUX_ROE,
+                         limiter=abi.LIMITER_MINMOD, timestep_set=abi.DT_FIXED, dt=1e-3)
+    s = Solver(c.config())
+    b = s.add_block((8, 8, 8), (0.125, 0.125, 0.125))
+    with pytest.raises(FvmError) as e:
+        s.step(1)  # nothing uploaded
+    assert e.value.code == 7  # FVM_ERR_STATE
+    with pytest.raises(FvmError) as e:
+        s.set_state(b + 5, np.zeros((5, 8, 8, 8)))
+    assert e.value.code == 1  # FVM_ERR_INVALID
+    s.set_state(b, c.states[0])
+    s.step(1)
+    with pytest.raises(FvmError) as e:
+        s.set_boundary(b, 7, abi.BC_PERIODIC)
+    assert e.value.code == 1
+    # a state with zero density is reported, not propagated silently
+    bad = c.states[0].copy()
+    bad[0, 4, 4, 4] = 0.0
+    s.set_state(b, bad)
+    with pytest.raises(FvmError) as e:
+        s.step(2)
+    assert e.value.code == 4  # FVM_ERR_NONFINITE
