@@ -50,7 +50,12 @@ struct StageCfg {
   static constexpr int WIN = H + 2;                        // z window: planes k-1 .. k+H
   static constexpr int WZ = RECON == RECON_WENO_ ? 2 : 1;  // warm-up planes before z0
   // R arrays first, then the FP64 staging of the cell's q0 / q_in / acc
-  static constexpr size_t r_elems = (size_t)(5 * PH * PW + NODEV * (NXN + NYN) + 5 * (NXF + NYF));
+  // WENO reads the plane only in phase A, so the face fluxes (phase B / C)
+  // share its storage; a barrier then separates phase C from the refill
+  static constexpr bool FAL = RECON == RECON_WENO_;
+  static constexpr size_t PF = FAL ? (5 * PH * PW > 5 * (NXF + NYF) ? 5 * PH * PW : 5 * (NXF + NYF))
+                                   : 5 * PH * PW + 5 * (NXF + NYF);
+  static constexpr size_t r_elems = (size_t)(PF + NODEV * (NXN + NYN));
   static constexpr size_t stage_off = (sizeof(R) * r_elems + 15) / 16 * 16;
   // The next plane's loads are prefetched asynchronously into shared memory
   // in the FP32 flux form and in small FP64 tiles; the large FP64 tiles,
@@ -225,8 +230,8 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);   // [5][PH][PW]   plane k + halo
-  R* sN = sP + 5 * PLANE;                   // [NODEV][NXN+NYN] x/y WENO nodes
-  R* sF = sN + C::NODEV * (C::NXN + C::NYN);  // [5][NXF+NYF]  x/y face fluxes
+  R* sN = sP + (C::FAL ? C::PF : 5 * PLANE);  // [NODEV][NXN+NYN] x/y WENO nodes
+  R* sF = C::FAL ? sP : sN + C::NODEV * (C::NXN + C::NYN);  // [5][NXF+NYF]  x/y face fluxes
   double* sQ = reinterpret_cast<double*>(smem_raw + C::stage_off);  // [2][5][NC] q0, q_in | acc
   double* sS = sQ + 2 * 5 * NC;                                       // [6][NT] residual / wave speed
   double* sX = sS + 6 * NT;                                           // [5][NPL] next plane's loads
@@ -665,6 +670,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       }
 
       // ---- carry, window shift and shared-memory refill ----------------------
+      if constexpr (C::FAL) __syncthreads();
       if constexpr (C::PSM) __pipeline_wait_prior(0);
       if (DIM == 3 && colt) {
 #pragma unroll
