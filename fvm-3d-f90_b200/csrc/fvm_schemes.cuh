@@ -114,20 +114,20 @@ __device__ __forceinline__ R muscl_right(R p1, R p2, R p3, const SchemeConst<R>&
 // textbook != 0: IS_1 with (u1-u3)^2 (Jiang & Shu); 0: (u1+u3)^2 as written.
 template <class R, bool EX>
 __device__ __forceinline__ R weno5(R u0, R u1, R u2, R u3, R u4, int textbook) {
-  const R q0 = R(1.0 / 3.0) * u0 - R(7.0 / 6.0) * u1 + R(11.0 / 6.0) * u2;
-  const R q1 = R(-1.0 / 6.0) * u1 + R(5.0 / 6.0) * u2 + R(1.0 / 3.0) * u3;
-  const R q2 = R(1.0 / 3.0) * u2 + R(5.0 / 6.0) * u3 - R(1.0 / 6.0) * u4;
-  const R a0 = u0 - R(2.0) * u1 + u2;
-  const R b0 = u0 - R(4.0) * u1 + R(3.0) * u2;
-  const R a1 = u1 - R(2.0) * u2 + u3;
-  const R b1 = textbook ? (u1 - u3) : (u1 + u3);
-  const R a2 = u2 - R(2.0) * u3 + u4;
-  const R b2 = R(3.0) * u2 - R(4.0) * u3 + u4;
-  const R IS0 = R(13.0 / 12.0) * (a0 * a0) + R(1.0 / 4.0) * (b0 * b0);
-  const R IS1 = R(13.0 / 12.0) * (a1 * a1) + R(1.0 / 4.0) * (b1 * b1);
-  const R IS2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
-  const R e0 = IS0 + R(1.0e-6), e1 = IS1 + R(1.0e-6), e2 = IS2 + R(1.0e-6);
   if constexpr (EX) {
+    const R q0 = R(1.0 / 3.0) * u0 - R(7.0 / 6.0) * u1 + R(11.0 / 6.0) * u2;
+    const R q1 = R(-1.0 / 6.0) * u1 + R(5.0 / 6.0) * u2 + R(1.0 / 3.0) * u3;
+    const R q2 = R(1.0 / 3.0) * u2 + R(5.0 / 6.0) * u3 - R(1.0 / 6.0) * u4;
+    const R a0 = u0 - R(2.0) * u1 + u2;
+    const R b0 = u0 - R(4.0) * u1 + R(3.0) * u2;
+    const R a1 = u1 - R(2.0) * u2 + u3;
+    const R b1 = textbook ? (u1 - u3) : (u1 + u3);
+    const R a2 = u2 - R(2.0) * u3 + u4;
+    const R b2 = R(3.0) * u2 - R(4.0) * u3 + u4;
+    const R IS0 = R(13.0 / 12.0) * (a0 * a0) + R(1.0 / 4.0) * (b0 * b0);
+    const R IS1 = R(13.0 / 12.0) * (a1 * a1) + R(1.0 / 4.0) * (b1 * b1);
+    const R IS2 = R(13.0 / 12.0) * (a2 * a2) + R(1.0 / 4.0) * (b2 * b2);
+    const R e0 = IS0 + R(1.0e-6), e1 = IS1 + R(1.0e-6), e2 = IS2 + R(1.0e-6);
     const R al0 = R(0.1) / (e0 * e0);
     const R al1 = R(0.6) / (e1 * e1);
     const R al2 = R(0.3) / (e2 * e2);
@@ -135,44 +135,61 @@ __device__ __forceinline__ R weno5(R u0, R u1, R u2, R u3, R u4, int textbook) {
     const R w0 = al0 / as, w1 = al1 / as, w2 = al2 / as;
     return w0 * q0 + w1 * q1 + w2 * q2;
   } else {
-    // omega_k = (c_k / d_k) / sum_j (c_j / d_j) = c_k prod_{j!=k} d_j / D
+    // The same mathematics in fewer operations. With the first differences
+    // Dij = uj - ui: q_k = u2 + delta_k (delta_0 = (5 D12 - 2 D01)/6,
+    // delta_1 = (D12 + 2 D23)/6, delta_2 = (4 D23 - D34)/6); a_k are the
+    // second differences, b_0 = 2 D12 + a_0, b_2 = a_2 - 2 D23. The
+    // smoothness indicators and eps are scaled by 4 (the weights only see
+    // their ratios): 4 (IS_k + eps) = 13/3 a_k^2 + b_k^2 + 4e-6. The weights
+    // are division-free, omega_k = c_k prod_{j!=k} d_j / D with d = e^2, and
+    // the result is u2 + sum omega_k delta_k.
+    const R D01 = u1 - u0, D12 = u2 - u1, D23 = u3 - u2, D34 = u4 - u3;
+    const R a0 = D12 - D01, a1 = D23 - D12, a2 = D34 - D23;
+    const R b0 = R(2.0) * D12 + a0;
+    const R b1 = textbook ? (D12 + D23) : (u1 + u3);
+    const R b2 = a2 - R(2.0) * D23;
+    const R e0 = (R(13.0 / 3.0) * a0) * a0 + (b0 * b0 + R(4.0e-6));
+    const R e1 = (R(13.0 / 3.0) * a1) * a1 + (b1 * b1 + R(4.0e-6));
+    const R e2 = (R(13.0 / 3.0) * a2) * a2 + (b2 * b2 + R(4.0e-6));
     const R d0 = e0 * e0, d1 = e1 * e1, d2 = e2 * e2;
-    const R t0 = R(0.1) * (d1 * d2);
-    const R t1 = R(0.6) * (d0 * d2);
-    const R t2 = R(0.3) * (d0 * d1);
-    return (t0 * q0 + t1 * q1 + t2 * q2) * rcp_(t0 + t1 + t2);
+    const R t0 = d1 * d2;
+    const R t1 = (R(6.0) * d0) * d2;
+    const R t2 = (R(3.0) * d0) * d1;
+    const R s0 = R(5.0 / 6.0) * D12 + R(-1.0 / 3.0) * D01;
+    const R s1 = R(1.0 / 3.0) * D23 + R(1.0 / 6.0) * D12;
+    const R s2 = R(2.0 / 3.0) * D23 + R(-1.0 / 6.0) * D34;
+    return (t0 * s0 + (t1 * s1 + t2 * s2)) * rcp_(t0 + (t1 + t2)) + u2;
   }
 }
 
 // Two WENO5 evaluations at once in packed FP32 (sm_100 f32x2 FMA / add /
-// multiply: one instruction per pair), for the FP32 flux form. Same formula as
-// weno5<float, false>; the pair shares `textbook`.
+// multiply: one instruction per pair), for the FP32 flux form: the
+// difference form of weno5<R, false>; the pair shares `textbook`.
 __device__ __forceinline__ float2 f2_(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 weno5x2(float2 u0, float2 u1, float2 u2, float2 u3, float2 u4, int textbook) {
-  const float2 q0 = __ffma2_rn(f2_(1.0f / 3.0f), u0, __ffma2_rn(f2_(-7.0f / 6.0f), u1, __fmul2_rn(f2_(11.0f / 6.0f), u2)));
-  const float2 q1 = __ffma2_rn(f2_(-1.0f / 6.0f), u1, __ffma2_rn(f2_(5.0f / 6.0f), u2, __fmul2_rn(f2_(1.0f / 3.0f), u3)));
-  const float2 q2 = __ffma2_rn(f2_(1.0f / 3.0f), u2, __ffma2_rn(f2_(5.0f / 6.0f), u3, __fmul2_rn(f2_(-1.0f / 6.0f), u4)));
-  const float2 a0 = __ffma2_rn(f2_(-2.0f), u1, __fadd2_rn(u0, u2));
-  const float2 b0 = __ffma2_rn(f2_(-4.0f), u1, __ffma2_rn(f2_(3.0f), u2, u0));
-  const float2 a1 = __ffma2_rn(f2_(-2.0f), u2, __fadd2_rn(u1, u3));
-  const float2 b1 = textbook ? __ffma2_rn(f2_(-1.0f), u3, u1) : __fadd2_rn(u1, u3);
-  const float2 a2 = __ffma2_rn(f2_(-2.0f), u3, __fadd2_rn(u2, u4));
-  const float2 b2 = __ffma2_rn(f2_(3.0f), u2, __ffma2_rn(f2_(-4.0f), u3, u4));
-  // IS_k + eps = 13/12 a^2 + 1/4 b^2 + 1e-6
-  const float2 e0 = __ffma2_rn(__fmul2_rn(f2_(13.0f / 12.0f), a0), a0,
-                               __ffma2_rn(__fmul2_rn(f2_(0.25f), b0), b0, f2_(1.0e-6f)));
-  const float2 e1 = __ffma2_rn(__fmul2_rn(f2_(13.0f / 12.0f), a1), a1,
-                               __ffma2_rn(__fmul2_rn(f2_(0.25f), b1), b1, f2_(1.0e-6f)));
-  const float2 e2 = __ffma2_rn(__fmul2_rn(f2_(13.0f / 12.0f), a2), a2,
-                               __ffma2_rn(__fmul2_rn(f2_(0.25f), b2), b2, f2_(1.0e-6f)));
+  const float2 m1 = f2_(-1.0f);
+  const float2 D01 = __ffma2_rn(m1, u0, u1), D12 = __ffma2_rn(m1, u1, u2);
+  const float2 D23 = __ffma2_rn(m1, u2, u3), D34 = __ffma2_rn(m1, u3, u4);
+  const float2 a0 = __ffma2_rn(m1, D01, D12), a1 = __ffma2_rn(m1, D12, D23), a2 = __ffma2_rn(m1, D23, D34);
+  const float2 b0 = __ffma2_rn(f2_(2.0f), D12, a0);
+  const float2 b1 = textbook ? __fadd2_rn(D12, D23) : __fadd2_rn(u1, u3);
+  const float2 b2 = __ffma2_rn(f2_(-2.0f), D23, a2);
+  // 4 (IS_k + eps) = 13/3 a_k^2 + b_k^2 + 4e-6
+  const float2 c = f2_(13.0f / 3.0f), eps = f2_(4.0e-6f);
+  const float2 e0 = __ffma2_rn(__fmul2_rn(c, a0), a0, __ffma2_rn(b0, b0, eps));
+  const float2 e1 = __ffma2_rn(__fmul2_rn(c, a1), a1, __ffma2_rn(b1, b1, eps));
+  const float2 e2 = __ffma2_rn(__fmul2_rn(c, a2), a2, __ffma2_rn(b2, b2, eps));
   const float2 d0 = __fmul2_rn(e0, e0), d1 = __fmul2_rn(e1, e1), d2 = __fmul2_rn(e2, e2);
-  // weights c_k / d_k normalised: scale all by 1/c_0 (t0 = d1 d2, t1 = 6 d0 d2, t2 = 3 d0 d1)
+  // weights c_k / d_k normalised by 1 / c_0: t0 = d1 d2, t1 = 6 d0 d2, t2 = 3 d0 d1
   const float2 t0 = __fmul2_rn(d1, d2);
   const float2 t1 = __fmul2_rn(__fmul2_rn(f2_(6.0f), d0), d2);
   const float2 t2 = __fmul2_rn(__fmul2_rn(f2_(3.0f), d0), d1);
-  const float2 num = __ffma2_rn(t0, q0, __ffma2_rn(t1, q1, __fmul2_rn(t2, q2)));
+  const float2 s0 = __ffma2_rn(f2_(5.0f / 6.0f), D12, __fmul2_rn(f2_(-1.0f / 3.0f), D01));
+  const float2 s1 = __ffma2_rn(f2_(1.0f / 3.0f), D23, __fmul2_rn(f2_(1.0f / 6.0f), D12));
+  const float2 s2 = __ffma2_rn(f2_(2.0f / 3.0f), D23, __fmul2_rn(f2_(-1.0f / 6.0f), D34));
+  const float2 num = __ffma2_rn(t0, s0, __ffma2_rn(t1, s1, __fmul2_rn(t2, s2)));
   const float2 den = __fadd2_rn(t0, __fadd2_rn(t1, t2));
-  return __fmul2_rn(num, make_float2(rcp_(den.x), rcp_(den.y)));
+  return __ffma2_rn(num, make_float2(rcp_(den.x), rcp_(den.y)), u2);
 }
 
 // The WENO node values of one stencil u[var][0..4]: wm (left-biased, value
