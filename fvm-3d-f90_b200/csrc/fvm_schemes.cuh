@@ -290,6 +290,30 @@ __device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, 
   const R ul[3] = {L.u, L.v, L.w};
   const R ur[3] = {Rs.u, Rs.v, Rs.w};
   const R l2r = lam2 * rho_b;
+  if constexpr (!EX) {
+    // the same flux with the wave sums collected: sum_k d_k r_k has
+    // momentum (d1+d234+d5) u_b + lam2 rho_b du (+ (d5-d1) c_b - lam2 rho_b dV
+    // along the normal) and energy (d1+d5) H_b + (d5-d1) c_b V_b
+    // + d234 q2_b / 2 + lam2 rho_b (u_b . du - V_b dV)
+    const R dsum = d1_0 + d234_0 + d5_0;
+    const R ddif = (d5_0 - d1_0) * c_b;
+    const R ml = L.r * Vc_l, mr = Rs.r * Vc_r;
+    F[0] = R(0.5) * ((ml + mr) - dsum);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      R diss = dsum * ub[m] + l2r * dd[m];
+      R phys = ml * ul[m] + mr * ur[m];
+      if (m == DIR) {
+        diss = diss + (ddif - l2r * dVl);
+        phys = phys + (L.p + Rs.p);
+      }
+      F[1 + m] = R(0.5) * (phys - diss);
+    }
+    const R ud = u_b * du + v_b * dv + w_b * dw - Vl_b * dVl;
+    const R de = (d1_0 + d5_0) * H_b + ddif * Vl_b + d234_0 * (R(0.5) * q2_b) + l2r * ud;
+    F[4] = R(0.5) * ((ml * H_l + mr * H_r) - de);
+    return;
+  }
   // mass
   F[0] = R(0.5) * ((L.r * Vc_l + Rs.r * Vc_r) - (d1_0 + d234_0 + d5_0));
   // momentum
