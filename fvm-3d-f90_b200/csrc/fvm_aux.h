@@ -30,6 +30,9 @@ struct StageKernelInfo {
   size_t smem = 0;
   int threads = 0;
   int tx = 0, ty = 0;
+  // tensor-map prefetch: the plane box is box_w x box_h cells (x, y), the z
+  // box tx x ty; the kernel expects StageArgs::tmap (0 = no tensor maps)
+  int tma = 0, box_w = 0, box_h = 0, halo = 0;
 };
 
 // Tile shapes compiled for every scheme (index -> TX x TY, minimum resident

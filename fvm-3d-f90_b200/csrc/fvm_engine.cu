@@ -16,10 +16,26 @@
 
 #include "fvm_engine.h"
 
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
+
 namespace fvm {
 
 namespace {
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled encode_fn() {
+  static PFN_cuTensorMapEncodeTiled fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
+  }
+  return fn;
+}
 
 // Split nz planes into chunks of at most L planes, all of nearly equal length
 // (lengths differ by at most one plane).
@@ -102,6 +118,11 @@ void Engine::release() {
   d_casemax_ = nullptr;
   d_staging_ = nullptr;
   staging_bytes_ = 0;
+  for (auto p : d_tmap_)
+    if (p) cudaFree(p);
+  d_tmap_.clear();
+  if (d_err_) cudaFree(d_err_);
+  d_err_ = nullptr;
   for (auto& b : blocks) {
     if (b.rhs_dev) cudaFree(b.rhs_dev);
     b.rhs_dev = nullptr;
@@ -907,6 +928,46 @@ int Engine::plan() {
     CK(cudaMemcpyAsync(d_pairs_, pairs.data(), sizeof(int64_t) * pairs.size(), cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d_counters_, 0, sizeof(int) * std::max(1, ncounters_), stream));
   CK(cudaMemsetAsync(d_partials_, 0, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size()), stream));
+
+  // -- tensor maps of the groups whose kernel prefetches with TMA: per block
+  //    and input role (A, B, C), the plane box and the z box over the block's
+  //    padded box as a 4D tensor (x, y, z, variable)
+  for (auto p : d_tmap_)
+    if (p) cudaFree(p);
+  d_tmap_.assign(groups.size(), nullptr);
+  if (!d_err_) CK(cudaMalloc(&d_err_, sizeof(int32_t)));
+  CK(cudaMemsetAsync(d_err_, 0, sizeof(int32_t), stream));
+  for (size_t g = 0; g < groups.size(); ++g) {
+    const Group& G = groups[g];
+    if (!G.k.tma) continue;
+    PFN_cuTensorMapEncodeTiled enc = encode_fn();
+    if (!enc) return fail(FVM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    std::vector<CUtensorMap> maps(blocks.size() * 3 * 2);
+    std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
+    for (int ci : live_cases) {
+      if (cases[ci].group != (int)g) continue;
+      for (int bi : cases[ci].blocks) {
+        const HBlock& b = blocks[bi];
+        const cuuint64_t dims[4] = {(cuuint64_t)b.px, (cuuint64_t)b.py, (cuuint64_t)b.pz, 5};
+        const cuuint64_t strides[3] = {(cuuint64_t)(b.sy * 8), (cuuint64_t)(b.sz * 8), (cuuint64_t)(cap_ * 8)};
+        const cuuint32_t box_p[4] = {(cuuint32_t)G.k.box_w, (cuuint32_t)G.k.box_h, 1, 5};
+        const cuuint32_t box_z[4] = {(cuuint32_t)G.k.tx, (cuuint32_t)G.k.ty, 1, 5};
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        for (int r = 0; r < 3; ++r) {
+          void* base = role_[r] + b.slab_off;
+          for (int w = 0; w < 2; ++w) {
+            const CUresult e = enc(&maps[((size_t)bi * 3 + r) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+                                   strides, w == 0 ? box_p : box_z, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (e != CUDA_SUCCESS) return fail(FVM_ERR_CUDA, "cuTensorMapEncodeTiled failed for a block");
+          }
+        }
+      }
+    }
+    CK(cudaMalloc(&d_tmap_[g], sizeof(CUtensorMap) * maps.size()));
+    CK(cudaMemcpyAsync(d_tmap_[g], maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, stream));
+  }
   CK(cudaStreamSynchronize(stream));
   planned_ = true;
   prepared_ = false;
@@ -964,6 +1025,8 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
       a.rq0 = ROLE_A;
       a.racc = (S == 4) ? ROLE_ACC : ROLE_A;
       a.last = (m == S) ? 1 : 0;
+      a.tmap = d_tmap_[g];
+      a.err = d_err_;
       void* args[] = {&a};
       cudaStream_t st = stream;
       if (fork) {
@@ -1126,7 +1189,10 @@ int Engine::read_case_state(int case_id, DevCaseState* out) {
   if (!d_state_ || case_id >= state_cap_ || cases[case_id].fresh)
     return fail(FVM_ERR_STATE, "no state uploaded yet");
   CK(cudaMemcpyAsync(out, d_state_ + case_id, sizeof(DevCaseState), cudaMemcpyDeviceToHost, stream));
+  int32_t err = 0;
+  if (d_err_) CK(cudaMemcpyAsync(&err, d_err_, sizeof err, cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
+  if (err) return fail(FVM_ERR_TIMEOUT, "a stage kernel's tensor copy did not arrive");
   return FVM_OK;
 }
 

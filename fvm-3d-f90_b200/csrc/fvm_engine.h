@@ -158,6 +158,8 @@ class Engine {
   int* d_counters_ = nullptr;
   int ncounters_ = 0;
   int vtask_off_ = 0, nvtask3_ = 0, nvtask2_ = 0;  // viscous tasks in d_tasks_
+  std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..C][plane, z] (null: no TMA)
+  int32_t* d_err_ = nullptr;          // kernel error flag (a tensor copy that did not arrive)
   unsigned long long* d_casemax_ = nullptr;
   double* d_staging_ = nullptr;
   size_t staging_bytes_ = 0;

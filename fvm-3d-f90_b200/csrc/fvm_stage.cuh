@@ -56,7 +56,7 @@ struct StageCfg {
   static constexpr size_t PF = FAL ? (5 * PH * PW > 5 * (NXF + NYF) ? 5 * PH * PW : 5 * (NXF + NYF))
                                    : 5 * PH * PW + 5 * (NXF + NYF);
   static constexpr size_t r_elems = (size_t)(PF + NODEV * (NXN + NYN));
-  static constexpr size_t stage_off = (sizeof(R) * r_elems + 15) / 16 * 16;
+  static constexpr size_t stage_off = (sizeof(R) * r_elems + 127) / 128 * 128;
   // The next plane's loads are prefetched asynchronously into shared memory
   // in the FP32 flux form and in small FP64 tiles; the large FP64 tiles,
   // whose shared arrays would then no longer fit twice on an SM, prefetch
@@ -66,7 +66,16 @@ struct StageCfg {
   // column's residual sums and wave-speed maximum and, with PSM, the prefetch
   // of the next plane's loaded cells [5][NPL] and, in 3D, of the z window's
   // next plane [5][NC], both as loaded (conservative FP64)
-  static constexpr int NPRE = PSM ? 5 * NPL + (DIM == 3 ? 5 * NC : 0) : 0;
+  // In 3D the prefetch is two tensor-map (TMA) boxes per plane, issued by
+  // one thread and completed on an mbarrier: the whole next plane with its
+  // x / y halo, [5][PH][TW] with TW = TX + 2H + 1 rounded up to even (the
+  // box starts on an even x, so its first coordinate is 16-byte aligned),
+  // and the z window's next plane, [5][TY][TX]; both padded to 128 bytes.
+  static constexpr bool TMA = PSM && DIM == 3;
+  static constexpr int TW = (TX + 2 * H + 2) / 2 * 2;
+  static constexpr int TPB = (5 * PH * TW + 15) / 16 * 16;
+  static constexpr int TZB = (5 * TY * TX + 15) / 16 * 16;
+  static constexpr int NPRE = TMA ? TPB + TZB : (PSM ? 5 * NPL + (DIM == 3 ? 5 * NC : 0) : 0);
   static constexpr size_t smem_bytes = stage_off + sizeof(double) * (2 * 5 * NC + 6 * NT + NPRE);
 };
 
@@ -104,6 +113,60 @@ __device__ __forceinline__ int xy_off(const BGeo& g, int x, int y) {
   if (y >= g.n1 && !(g.mask & 8)) y = g.n1 - 1;
   return x + y * g.sy;
 }
+// The same rule returning the clamped (x, y).
+__device__ __forceinline__ void xy_clamp(const BGeo& g, int& x, int& y) {
+  x = max(x, -kGhost);
+  x = min(x, g.n0 + kGhost - 1);
+  y = max(y, -kGhost);
+  y = min(y, g.n1 + kGhost - 1);
+  if (x < 0 && !(g.mask & 1)) x = 0;
+  if (x >= g.n0 && !(g.mask & 2)) x = g.n0 - 1;
+  if (y < 0 && !(g.mask & 4)) y = 0;
+  if (y >= g.n1 && !(g.mask & 8)) y = g.n1 - 1;
+}
+
+// ---- tensor-map copies and mbarriers (sm_90+ PTX; no cluster multicast)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase `parity` of b to complete; gives up after a bounded
+// number of polls (each poll itself waits a hardware-defined while) and
+// returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+  for (int i = 0; i < (1 << 20); ++i)
+    if (mbar_try_wait(b, parity)) return true;
+  return false;
+}
+// 4D tiled tensor copy global -> this CTA's shared memory, completing on b.
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(b))
+      : "memory");
+}
+
 __device__ __forceinline__ int z_clamp(const BGeo& g, int z) {
   z = max(z, -kGhost);
   z = min(z, g.n2 + kGhost - 1);
@@ -228,7 +291,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
   constexpr int H = C::H, NT = C::NT, NC = C::NC, PW = C::PW, PH = C::PH;
   constexpr int PLANE = PH * PW;
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   R* sP = reinterpret_cast<R*>(smem_raw);   // [5][PH][PW]   plane k + halo
   R* sN = sP + (C::FAL ? C::PF : 5 * PLANE);  // [NODEV][NXN+NYN] x/y WENO nodes
   R* sF = C::FAL ? sP : sN + C::NODEV * (C::NXN + C::NYN);  // [5][NXF+NYF]  x/y face fluxes
@@ -236,13 +299,25 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
   double* sS = sQ + 2 * 5 * NC;                                       // [6][NT] residual / wave speed
   double* sX = sS + 6 * NT;                                           // [5][NPL] next plane's loads
   double* sZ = sX + 5 * C::NPL;                                       // [5][NC] z window's next plane (3D)
+  double* sTP = sS + 6 * NT;                                          // TMA: [5][PH][TW] next plane
+  double* sTZ = sTP + C::TPB;                                         // TMA: [5][TY][TX] z window's next plane
   __shared__ double s_red[6 * (NT / 32)];
   __shared__ int s_task;
+  __shared__ __align__(8) uint64_t s_mbar[2];  // TMA: plane box, z box
+  uint32_t ph_p = 0, ph_z = 0;                 // TMA: expected phase parity of each mbarrier
 
   const int tid = threadIdx.x;
   // column threads own a z column; the others (whole warps) skip all z work
   const bool colt = (NC == NT) || tid < NC;
   const int tx = tid % TX, ty = tid / TX;
+  if constexpr (C::TMA) {
+    if (tid == 0) {
+      mbar_init(&s_mbar[0], 1);
+      mbar_init(&s_mbar[1], 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+  }
 
   for (;;) {
     if (tid == 0) s_task = atomicAdd(a.counter, 1);
@@ -294,8 +369,11 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 #pragma unroll
       for (int v = 0; v < 6; ++v) sS[v * NT + tid] = 0.0;
 
-    // loop-invariant (x, y) parts of this thread's plane loads
+    // loop-invariant (x, y) parts of this thread's plane loads: the global
+    // offset, or with TMA the index of the (clamped) cell in the plane box
     int lxy[C::NPS], lsp[C::NPS];
+    // TMA: the plane box starts at padded x = xs (even), padded y = T.y0 + kGhost - H
+    const int xs = (T.x0 + kPadX - H) & ~1;
 #pragma unroll
     for (int sidx = 0; sidx < C::NPS; ++sidx) {
       const int w = tid + sidx * NT;
@@ -305,10 +383,25 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         int xx, yy;
         plane_cell<TX, TY, H, DIM>(w, xx, yy);
         lsp[sidx] = yy * PW + xx;
-        lxy[sidx] = xy_off(G, T.x0 + xx - H, T.y0 + yy - H);
+        if constexpr (C::TMA) {
+          int x = T.x0 + xx - H, y = T.y0 + yy - H;
+          xy_clamp(G, x, y);
+          lxy[sidx] = (y - T.y0 + H) * C::TW + (x + kPadX - xs);
+        } else {
+          lxy[sidx] = xy_off(G, T.x0 + xx - H, T.y0 + yy - H);
+        }
       }
     }
     const int cxy = xy_off(G, gx, gy);
+    // TMA: index of this column's (clamped) cell in the z box
+    int zsrc = 0;
+    if constexpr (C::TMA) {
+      int x = gx, y = gy;
+      xy_clamp(G, x, y);
+      zsrc = (y - T.y0) * TX + (x - T.x0);
+    }
+    const CUtensorMap* tmp = nullptr;
+    if constexpr (C::TMA) tmp = a.tmap + ((int64_t)T.blk * 3 + a.rin) * 2;
 
     // ---- z window (3D) --------------------------------------------------
     R zw[C::WIN][5];
@@ -349,7 +442,18 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       // own copies), else into registers.
       double pre[C::PSM ? 1 : C::NPS][5];
       double zpre[5];
-      if (more_xy) {
+      if constexpr (C::TMA) {
+        if (tid == 0) {
+          if (more_xy) {
+            mbar_expect_tx(&s_mbar[0], sizeof(double) * 5 * PH * C::TW);
+            tma_load_4d(sTP, tmp, xs, T.y0 + kGhost - H, k + 1 + kGhost, 0, &s_mbar[0]);
+          }
+          if (more) {
+            mbar_expect_tx(&s_mbar[1], sizeof(double) * 5 * TY * TX);
+            tma_load_4d(sTZ, tmp + 1, T.x0 + kPadX, T.y0 + kGhost, z_clamp(G, k + H + 1) + kGhost, 0, &s_mbar[1]);
+          }
+        }
+      } else if (more_xy) {
 #pragma unroll
         for (int sidx = 0; sidx < C::NPS; ++sidx) {
           if (lsp[sidx] >= 0) {
@@ -364,7 +468,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
           }
         }
       }
-      if constexpr (DIM == 3) {
+      if constexpr (DIM == 3 && !C::TMA) {
         if (more && colt) {
           const double* src = qin + (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz;
           if constexpr (C::PSM) {
@@ -375,7 +479,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
           }
         }
       }
-      if constexpr (C::PSM) __pipeline_commit();
+      if constexpr (C::PSM && !C::TMA) __pipeline_commit();
 
       // ---- the cell's RK operands of plane k, copied asynchronously into
       // shared memory; phase C waits for this thread's own copies only.
@@ -671,7 +775,25 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 
       // ---- carry, window shift and shared-memory refill ----------------------
       if constexpr (C::FAL) __syncthreads();
-      if constexpr (C::PSM) __pipeline_wait_prior(0);
+      if constexpr (C::PSM && !C::TMA) __pipeline_wait_prior(0);
+      if constexpr (C::TMA) {
+        // every thread waits for the boxes issued at the top of this plane
+        bool ok = true;
+        if (more) {
+          ok = mbar_wait(&s_mbar[1], ph_z);
+          ph_z ^= 1;
+        }
+        if (more_xy && ok) {
+          ok = mbar_wait(&s_mbar[0], ph_p);
+          ph_p ^= 1;
+        }
+        if (!ok) {
+          // a copy did not arrive: report it and leave (every thread of the
+          // CTA polls the same barrier, so they leave together)
+          if (tid == 0) atomicExch(a.err, 1);
+          return;
+        }
+      }
       if (DIM == 3 && colt) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) zFprev[v] = zF[v];
@@ -681,7 +803,10 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 #pragma unroll
           for (int v = 0; v < 5; ++v) zw[s][v] = zw[s + 1][v];
         if (more) {
-          if constexpr (C::PSM) {
+          if constexpr (C::TMA) {
+#pragma unroll
+            for (int v = 0; v < 5; ++v) zpre[v] = sTZ[v * (TX * TY) + zsrc];
+          } else if constexpr (C::PSM) {
 #pragma unroll
             for (int v = 0; v < 5; ++v) zpre[v] = sZ[v * NC + tid];
           }
@@ -698,7 +823,10 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         for (int sidx = 0; sidx < C::NPS; ++sidx) {
           if (lsp[sidx] >= 0) {
             double q[5];
-            if constexpr (C::PSM) {
+            if constexpr (C::TMA) {
+#pragma unroll
+              for (int v = 0; v < 5; ++v) q[v] = sTP[v * (PH * C::TW) + lxy[sidx]];
+            } else if constexpr (C::PSM) {
               const int w = tid + sidx * NT;
 #pragma unroll
               for (int v = 0; v < 5; ++v) q[v] = sX[v * C::NPL + w];

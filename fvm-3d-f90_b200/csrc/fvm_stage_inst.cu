@@ -26,6 +26,10 @@ static bool fill(StageKernelInfo* out) {
   out->threads = Cfg::NT;
   out->tx = TX;
   out->ty = TY;
+  out->tma = Cfg::TMA ? 1 : 0;
+  out->box_w = Cfg::TW;
+  out->box_h = Cfg::PH;
+  out->halo = Cfg::H;
   return true;
 }
 
