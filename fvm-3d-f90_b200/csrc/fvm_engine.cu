@@ -8,6 +8,7 @@
 // global_error.f90:18-33). No CUDA call is made before the first state upload
 // or step, so configuration errors surface without a GPU.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -399,6 +400,14 @@ int Engine::resolve(int blk, int64_t x[3], int* out_blk) const {
 }
 
 // ---------------------------------------------------------------- planning
+int Engine::set_drop_copies(bool on) {
+  if (drop_copies_ != on) {
+    drop_copies_ = on;
+    planned_ = false;  // the step graph carries the flag in its kernel arguments
+  }
+  return FVM_OK;
+}
+
 int Engine::set_tuning(int case_id, int tile, int zchunk) {
   if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
   if (tile < -1 || tile >= kNumTiles) return fail(FVM_ERR_INVALID, "bad tile index");
@@ -1027,6 +1036,7 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
       a.last = (m == S) ? 1 : 0;
       a.tmap = d_tmap_[g];
       a.err = d_err_;
+      a.drop_copies = drop_copies_ ? 1 : 0;
       void* args[] = {&a};
       cudaStream_t st = stream;
       if (fork) {
@@ -1133,6 +1143,11 @@ int Engine::set_state(int blk, const double* q) {
   CK(cudaMemcpyAsync(d_staging_, q, bytes, cudaMemcpyHostToDevice, stream));
   CK(launch_unpack(role_[ROLE_A] + b.slab_off + b.org, cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
                    d_staging_, stream));
+  // a new state clears the case's error status (NaN / divergence of an
+  // earlier state)
+  if (d_state_ && b.case_id < state_cap_ && !cases[b.case_id].fresh)
+    CK(cudaMemsetAsync(reinterpret_cast<char*>(d_state_ + b.case_id) + offsetof(DevCaseState, status), 0,
+                       sizeof(int32_t), stream));
   CK(cudaStreamSynchronize(stream));
   prepared_ = false;
   return FVM_OK;
@@ -1192,7 +1207,12 @@ int Engine::read_case_state(int case_id, DevCaseState* out) {
   int32_t err = 0;
   if (d_err_) CK(cudaMemcpyAsync(&err, d_err_, sizeof err, cudaMemcpyDeviceToHost, stream));
   CK(cudaStreamSynchronize(stream));
-  if (err) return fail(FVM_ERR_TIMEOUT, "a stage kernel's tensor copy did not arrive");
+  if (err) {
+    // reported once; the context stays usable (the state of this step is not)
+    CK(cudaMemsetAsync(d_err_, 0, sizeof(int32_t), stream));
+    CK(cudaStreamSynchronize(stream));
+    return fail(FVM_ERR_TIMEOUT, "a stage kernel's tensor copy did not arrive within 1 s");
+  }
   return FVM_OK;
 }
 
@@ -1452,6 +1472,11 @@ int fvm_profile_step(fvm_ctx* ctx, float* ms, int32_t* kinds, int cap, int* n) {
   int rc = ctx->eng.profile_step(ms, k.data(), cap, n);
   for (int i = 0; i < *n; ++i) kinds[i] = k[i];
   return rc;
+}
+
+int fvm_test_drop_tensor_copies(fvm_ctx* ctx, int on) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.set_drop_copies(on != 0);
 }
 
 int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n) {

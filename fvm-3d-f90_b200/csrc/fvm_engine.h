@@ -92,6 +92,8 @@ class Engine {
   int step(int nsteps);
   int read_case_state(int case_id, DevCaseState* out);
 
+  // Test hook of the tensor-copy timeout path (see fvm_test_drop_tensor_copies).
+  int set_drop_copies(bool on);
   // Tuning hooks (autotuner): force tile shape / z chunk of a case.
   int set_tuning(int case_id, int tile, int zchunk);
   // Mean device time of `reps` graph-launched steps (ms).
@@ -160,6 +162,7 @@ class Engine {
   int vtask_off_ = 0, nvtask3_ = 0, nvtask2_ = 0;  // viscous tasks in d_tasks_
   std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..C][plane, z] (null: no TMA)
   int32_t* d_err_ = nullptr;          // kernel error flag (a tensor copy that did not arrive)
+  bool drop_copies_ = false;          // test hook: tensor copies armed but not issued
   unsigned long long* d_casemax_ = nullptr;
   double* d_staging_ = nullptr;
   size_t staging_bytes_ = 0;

@@ -149,12 +149,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for the phase `parity` of b to complete; gives up after a bounded
-// number of polls (each poll itself waits a hardware-defined while) and
-// returns false.
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Wait for the phase `parity` of b to complete; gives up after one second
+// (or a bounded number of polls) and returns false.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-  for (int i = 0; i < (1 << 20); ++i)
+  if (mbar_try_wait(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (int i = 0; i < (1 << 26); ++i) {
     if (mbar_try_wait(b, parity)) return true;
+    if (global_ns() - t0 > 1000000000ull) return false;
+  }
   return false;
 }
 // 4D tiled tensor copy global -> this CTA's shared memory, completing on b.
@@ -446,7 +454,9 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         if (tid == 0) {
           if (more_xy) {
             mbar_expect_tx(&s_mbar[0], sizeof(double) * 5 * PH * C::TW);
-            tma_load_4d(sTP, tmp, xs, T.y0 + kGhost - H, k + 1 + kGhost, 0, &s_mbar[0]);
+            // a.drop_copies (a test of the timeout path): the barrier is armed
+            // but the copy never issued, so the wait below runs out
+            if (!a.drop_copies) tma_load_4d(sTP, tmp, xs, T.y0 + kGhost - H, k + 1 + kGhost, 0, &s_mbar[0]);
           }
           if (more) {
             mbar_expect_tx(&s_mbar[1], sizeof(double) * 5 * TY * TX);

@@ -92,6 +92,7 @@ struct StageArgs {
   // (null for kernels that load with per-thread copies)
   const CUtensorMap* tmap;
   int32_t* err;                // set to 1 when a tensor copy does not arrive
+  int32_t drop_copies;         // test of the timeout path: arm the barrier, skip the copy
 };
 
 }  // namespace fvm

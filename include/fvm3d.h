@@ -237,6 +237,12 @@ int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step);
  * number of kernels one (graph-captured) time step launches. */
 int fvm_profile_step(fvm_ctx* ctx, float* ms, int32_t* kinds, int cap, int* n);
 int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n);
+/* Test hook of the failure path; no counterpart in the reference. With on
+ * != 0 the stage kernels that fetch planes through tensor copies arm their
+ * barrier but skip the copy, so their bounded wait (1 s) runs out: the next
+ * fvm_step / fvm_case_state returns FVM_ERR_TIMEOUT once, and the context
+ * stays usable (upload a state again after turning the hook off). */
+int fvm_test_drop_tensor_copies(fvm_ctx* ctx, int on);
 
 /* Residual norms of one block's rhs in device memory, as
  * ClassIteration%compute_residual_sub (class_iteration.f90, file-local
