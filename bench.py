@@ -35,7 +35,7 @@ sys.path.insert(0, PKG)
 
 METRIC = "Gcell-stage/s FP64 plain vs FP32-batched at L1 err<=1e-6; served p50/p99 latency"
 UNIT = "Gcell-stage/s"
-STAGE_TRAFFIC_FP32 = 403.33e6  # bytes per stage launch, ncu dram__bytes_read.sum + dram__bytes_write.sum
+STAGE_TRAFFIC_FP32 = 403.53e6  # bytes per stage launch, ncu dram__bytes_read.sum + dram__bytes_write.sum
 WORKLOAD = "isentropic vortex 3D Euler, periodic [-5,5]^3, 8 uneven blocks, 128^3 = 2,097,152 cells, WENO5 + AUSM, RK4, CFL 0.5"
 
 
