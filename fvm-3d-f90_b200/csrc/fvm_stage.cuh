@@ -10,8 +10,11 @@
 // A task is a TX x TY column tile of one block over a z range [z0, z1).
 // The CTA marches the tile along z:
 //   * the z stencil of each column lives in a register window (planes
-//     k-1 .. k+H), refilled by one coalesced plane load per step;
+//     k-1 .. k+H), refilled from the next plane each step;
 //   * plane k with its x/y halo (H cells, no corners) sits in shared memory;
+//     in 3D the next plane and the z window's next plane arrive as TMA
+//     tensor boxes while the current plane is computed (the large FP64
+//     tiles prefetch into registers instead);
 //   * each face flux is computed once and kept in shared memory (x, y) or in
 //     registers (z), and the cell's rhs is the reference's sum
 //       rhs = ((0 - dFx/dx) - dFy/dy) - dFz/dz.
