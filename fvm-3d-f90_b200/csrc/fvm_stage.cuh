@@ -529,7 +529,73 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
             if (!admissible(zWcur)) zWcur = pc;
           }
         }
-        if (do_xy) {
+        if constexpr (sizeof(R) == 4 && !TB) {
+         if (do_xy) {
+          // FP32, left-biased nodes only: a node's five variables fill two
+          // and a half f32x2 pairs, so two nodes are taken together and their
+          // fifth variables share one pair
+          constexpr int NN = C::NXN + C::NYN;
+          auto load_node = [&](int w, R (&u)[5][5]) {
+            if (w < C::NXN) {
+              const int c = w % (TX + 2) - 1, row = w / (TX + 2);
+              const int base = (H + row) * PW + (H + c - 2);
+#pragma unroll
+              for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s];
+            } else {
+              const int w2 = w - C::NXN;
+              const int col = w2 % TX, c = w2 / TX - 1;
+              const int base = (H + c - 2) * PW + (H + col);
+#pragma unroll
+              for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s * PW];
+            }
+          };
+          auto pair = [&](const R (&x)[5], const R (&y)[5]) {
+            return weno5x2(make_float2(x[0], y[0]), make_float2(x[1], y[1]), make_float2(x[2], y[2]),
+                           make_float2(x[3], y[3]), make_float2(x[4], y[4]), K.textbook);
+          };
+          auto first4 = [&](const R (&u)[5][5], R (&wm)[5]) {
+            const float2 r01 = pair(u[0], u[1]), r23 = pair(u[2], u[3]);
+            wm[0] = r01.x;
+            wm[1] = r01.y;
+            wm[2] = r23.x;
+            wm[3] = r23.y;
+          };
+          auto finish = [&](int w, const R (&u)[5][5], const R (&wm)[5]) {
+            Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
+            if (K.textbook && !admissible(pm))
+              pm = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
+            sN[0 * NN + w] = pm.r;
+            sN[1 * NN + w] = pm.u;
+            sN[2 * NN + w] = pm.v;
+            sN[3 * NN + w] = pm.w;
+            sN[4 * NN + w] = pm.p;
+          };
+          for (int w = tid; w < NN; w += 2 * NT) {
+            R ua[5][5], wa[5];
+            load_node(w, ua);
+            first4(ua, wa);
+            const int wb = w + NT;
+            if (wb < NN) {
+              R ub[5][5], wb4[5];
+              load_node(wb, ub);
+              first4(ub, wb4);
+              const float2 r4 = pair(ua[4], ub[4]);
+              wa[4] = r4.x;
+              wb4[4] = r4.y;
+              finish(w, ua, wa);
+              finish(wb, ub, wb4);
+            } else {
+              wa[4] = pair(ua[4], ua[4]).x;
+              finish(w, ua, wa);
+            }
+          }
+          __syncthreads();
+         }
+        } else if (do_xy) {
           for (int w = tid; w < C::NXN + C::NYN; w += NT) {
             R u[5][5];
             if (w < C::NXN) {
