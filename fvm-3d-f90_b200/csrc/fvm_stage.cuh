@@ -510,31 +510,13 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       // ---- phase A: WENO nodes --------------------------------------------
       Prim5<R> zWcur, zWm_cur;
       if constexpr (RECON == RECON_WENO_) {
-        if (DIM == 3 && colt) {
-          // node of plane k+1 from planes k-1 .. k+3 (window slots 0..4)
-          R wm[5], wp[5], u[5][5];
-#pragma unroll
-          for (int v = 0; v < 5; ++v)
-#pragma unroll
-            for (int s = 0; s < 5; ++s) u[v][s] = zw[s][v];
-          weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
-          zWm_cur = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
-          if (TB)
-            zWcur = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
-          else
-            zWcur = zWm_cur;
-          if (K.textbook && !(admissible(zWm_cur) && admissible(zWcur))) {
-            const Prim5<R> pc = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
-            if (!admissible(zWm_cur)) zWm_cur = pc;
-            if (!admissible(zWcur)) zWcur = pc;
-          }
-        }
         if constexpr (sizeof(R) == 4 && !TB) {
-         if (do_xy) {
-          // FP32, left-biased nodes only: a node's five variables fill two
-          // and a half f32x2 pairs, so two nodes are taken together and their
-          // fifth variables share one pair
+          // FP32, left-biased nodes only. A node's five variables fill two and
+          // a half f32x2 pairs, so nodes are taken in twos and their fifth
+          // variables share a pair: the thread's first two x / y nodes, and
+          // its third one with the z node of its column (or each alone).
           constexpr int NN = C::NXN + C::NYN;
+          static_assert(NN >= NT && NN <= 3 * NT, "x/y node items per thread");
           auto load_node = [&](int w, R (&u)[5][5]) {
             if (w < C::NXN) {
               const int c = w % (TX + 2) - 1, row = w / (TX + 2);
@@ -574,28 +556,86 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
             sN[3 * NN + w] = pm.w;
             sN[4 * NN + w] = pm.p;
           };
-          for (int w = tid; w < NN; w += 2 * NT) {
-            R ua[5][5], wa[5];
-            load_node(w, ua);
-            first4(ua, wa);
-            const int wb = w + NT;
-            if (wb < NN) {
-              R ub[5][5], wb4[5];
-              load_node(wb, ub);
-              first4(ub, wb4);
-              const float2 r4 = pair(ua[4], ub[4]);
-              wa[4] = r4.x;
-              wb4[4] = r4.y;
-              finish(w, ua, wa);
-              finish(wb, ub, wb4);
-            } else {
-              wa[4] = pair(ua[4], ua[4]).x;
-              finish(w, ua, wa);
+          // z node of plane k+1 from planes k-1 .. k+3 (window slots 0..4)
+          const bool hz = DIM == 3 && colt;
+          R uz4[5], wz[5];
+          bool zpaired = false;
+          if (hz) {
+            R uz[5][5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v)
+#pragma unroll
+              for (int s = 0; s < 5; ++s) uz[v][s] = zw[s][v];
+            first4(uz, wz);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) uz4[s] = uz[4][s];
+          }
+          if (do_xy) {
+            const int wa = tid, wb = tid + NT, wc = tid + 2 * NT;
+            {
+              R ua[5][5], va[5];
+              load_node(wa, ua);
+              first4(ua, va);
+              if (wb < NN) {
+                R ub[5][5], vb[5];
+                load_node(wb, ub);
+                first4(ub, vb);
+                const float2 r4 = pair(ua[4], ub[4]);
+                va[4] = r4.x;
+                vb[4] = r4.y;
+                finish(wa, ua, va);
+                finish(wb, ub, vb);
+              } else {
+                va[4] = pair(ua[4], ua[4]).x;
+                finish(wa, ua, va);
+              }
+            }
+            if (wc < NN) {
+              R uc[5][5], vc[5];
+              load_node(wc, uc);
+              first4(uc, vc);
+              if (hz) {
+                const float2 r4 = pair(uz4, uc[4]);
+                wz[4] = r4.x;
+                vc[4] = r4.y;
+                zpaired = true;
+              } else {
+                vc[4] = pair(uc[4], uc[4]).x;
+              }
+              finish(wc, uc, vc);
             }
           }
-          __syncthreads();
-         }
-        } else if (do_xy) {
+          if (hz) {
+            if (!zpaired) wz[4] = pair(uz4, uz4).x;
+            zWm_cur = cons2prim<R, EX>(wz[0], wz[1], wz[2], wz[3], wz[4], K.gm1);
+            zWcur = zWm_cur;
+            if (K.textbook && !admissible(zWm_cur)) {
+              zWm_cur = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
+              zWcur = zWm_cur;
+            }
+          }
+          if (do_xy) __syncthreads();
+        } else {
+        if (DIM == 3 && colt) {
+          // node of plane k+1 from planes k-1 .. k+3 (window slots 0..4)
+          R wm[5], wp[5], u[5][5];
+#pragma unroll
+          for (int v = 0; v < 5; ++v)
+#pragma unroll
+            for (int s = 0; s < 5; ++s) u[v][s] = zw[s][v];
+          weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
+          zWm_cur = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
+          if (TB)
+            zWcur = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
+          else
+            zWcur = zWm_cur;
+          if (K.textbook && !(admissible(zWm_cur) && admissible(zWcur))) {
+            const Prim5<R> pc = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
+            if (!admissible(zWm_cur)) zWm_cur = pc;
+            if (!admissible(zWcur)) zWcur = pc;
+          }
+        }
+        if (do_xy) {
           for (int w = tid; w < C::NXN + C::NYN; w += NT) {
             R u[5][5];
             if (w < C::NXN) {
@@ -636,6 +676,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
             }
           }
           __syncthreads();
+        }
         }
       }
 
