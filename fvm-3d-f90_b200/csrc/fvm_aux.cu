@@ -201,13 +201,24 @@ __device__ __forceinline__ int64_t vcell(const DevBlock& B, int x, int y, int z)
   return x + (int64_t)y * B.sy + (int64_t)z * B.sz;
 }
 
+// EX: the exact expression trees (divisions); otherwise one reciprocal.
+template <bool EX>
 __device__ __forceinline__ VPrim vprim(const double* q, int64_t o, int64_t vs, double gm1) {
-  Prim5<double> p = cons2prim<double, true>(q[o], q[o + vs], q[o + 2 * vs], q[o + 3 * vs], q[o + 4 * vs], gm1);
   VPrim r;
-  r.u = p.u;
-  r.v = p.v;
-  r.w = p.w;
-  r.th = p.p / p.r;
+  if constexpr (EX) {
+    Prim5<double> p = cons2prim<double, true>(q[o], q[o + vs], q[o + 2 * vs], q[o + 3 * vs], q[o + 4 * vs], gm1);
+    r.u = p.u;
+    r.v = p.v;
+    r.w = p.w;
+    r.th = p.p / p.r;
+  } else {
+    const double q0 = q[o], q1 = q[o + vs], q2 = q[o + 2 * vs], q3 = q[o + 3 * vs], q4 = q[o + 4 * vs];
+    const double ir = 1.0 / q0;
+    r.u = q1 * ir;
+    r.v = q2 * ir;
+    r.w = q3 * ir;
+    r.th = gm1 * (q4 - 0.5 * (q1 * r.u + q2 * r.v + q3 * r.w)) * ir;
+  }
   return r;
 }
 
@@ -219,20 +230,26 @@ __device__ __forceinline__ double vcomp(const VPrim& p, int m) {
 // cells L and R. tg[d] holds, for each tangential axis d != dir, the cells
 // L + e_d, L - e_d, R + e_d, R - e_d; the tangential gradient is the mean of
 // the two central differences.
+// EX divides by the cell sizes; otherwise multiplies by their reciprocals.
+template <bool EX>
 __device__ __forceinline__ void visc_flux(const VPrim& L, const VPrim& R, const VPrim (*tg)[4], int dir,
-                                          const double dr[3], double mu, double kq, int idim, double G[5]) {
+                                          const double dr[3], const double idr[3], double mu, double kq, int idim,
+                                          double G[5]) {
   double grad[4][3];
   for (int m = 0; m < 4; ++m)
     for (int d = 0; d < 3; ++d) grad[m][d] = 0.0;
-  for (int m = 0; m < 4; ++m) grad[m][dir] = (vcomp(R, m) - vcomp(L, m)) / dr[dir];
+  for (int m = 0; m < 4; ++m)
+    grad[m][dir] = EX ? (vcomp(R, m) - vcomp(L, m)) / dr[dir] : (vcomp(R, m) - vcomp(L, m)) * idr[dir];
   for (int d = 0; d < idim; ++d) {
     if (d == dir) continue;
     const VPrim& lp = tg[d][0];
     const VPrim& lm = tg[d][1];
     const VPrim& rp = tg[d][2];
     const VPrim& rm = tg[d][3];
-    for (int m = 0; m < 4; ++m)
-      grad[m][d] = ((vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m))) / (4.0 * dr[d]);
+    for (int m = 0; m < 4; ++m) {
+      const double s = (vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m));
+      grad[m][d] = EX ? s / (4.0 * dr[d]) : s * (0.25 * idr[d]);
+    }
   }
   const double div = grad[0][0] + grad[1][1] + grad[2][2];
   const double uf[3] = {0.5 * (L.u + R.u), 0.5 * (L.v + R.v), 0.5 * (L.w + R.w)};
@@ -253,22 +270,20 @@ __device__ __forceinline__ void visc_flux(const VPrim& L, const VPrim& R, const 
 // one-cell halo sit in a shared-memory ring; each x / y face flux of plane k
 // is computed once into shared memory, each z face once per column (the lower
 // one carried in registers). V = (dGx + dGy) + dGz as in the per-cell form.
-template <int TX, int TY, int IDIM>
-__global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* blocks, const DevCase* cases,
-                                                          const Task* tasks, int role) {
-  constexpr int NT = TX * TY, PX = TX + 2, PY = TY + 2, PL = PX * PY;
-  constexpr int NR = IDIM == 3 ? 3 : 1;
+// EX: the exact form the exact-FP64 cases need for parity with the oracle;
+// the other precision forms multiply by reciprocals instead of dividing.
+template <int TX, int TY, int IDIM, bool EX>
+__device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase& C, const Task& T, int role,
+                                               VPrim (*sp)[(TX + 2) * (TY + 2)],
+                                               double (*sg)[(TX + 1) * TY + TX * (TY + 1)]) {
+  constexpr int NT = TX * TY, PX = TX + 2;
   constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1), NF = NXF + NYF;
-  __shared__ VPrim sp[NR][PL];
-  __shared__ double sg[4][NF];
-
-  const Task T = tasks[blockIdx.x];
-  const DevBlock& B = blocks[T.blk];
-  const DevCase& C = cases[B.case_id];
+  constexpr int PL = (TX + 2) * (TY + 2);
   const double* q = B.q[role];
   const int64_t vs = B.vs;
   const double gm1 = C.gm1, mu = C.mu, kq = C.kq;
   const double dr[3] = {B.dr[0], B.dr[1], B.dr[2]};
+  const double idr[3] = {B.inv_dr[0], B.inv_dr[1], B.inv_dr[2]};
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const bool act = (T.x0 + tx < B.n[0]) && (T.y0 + ty < B.n[1]);
   auto slot = [](int z) { return IDIM == 3 ? ((z % 3) + 3) % 3 : 0; };
@@ -279,7 +294,7 @@ __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* block
     for (int w = tid; w < PL; w += NT) {
       const int x = min(max(T.x0 + w % PX - 1, -1), B.n[0]);
       const int y = min(max(T.y0 + w / PX - 1, -1), B.n[1]);
-      dst[w] = vprim(q, vcell(B, x, y, z), vs, gm1);
+      dst[w] = vprim<EX>(q, vcell(B, x, y, z), vs, gm1);
     }
   };
   auto P = [&](int z, int x, int y) -> const VPrim& { return sp[slot(z)][(y + 1) * PX + (x + 1)]; };
@@ -294,7 +309,7 @@ __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* block
     tg[1][1] = P(z, tx, ty - 1);
     tg[1][2] = P(z + 1, tx, ty + 1);
     tg[1][3] = P(z + 1, tx, ty - 1);
-    visc_flux(P(z, tx, ty), P(z + 1, tx, ty), tg, 2, dr, mu, kq, 3, G);
+    visc_flux<EX>(P(z, tx, ty), P(z + 1, tx, ty), tg, 2, dr, idr, mu, kq, 3, G);
   };
 
   double Gzl[5] = {0, 0, 0, 0, 0}, Gzr[5] = {0, 0, 0, 0, 0};
@@ -320,7 +335,7 @@ __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* block
           tg[2][2] = P(k + 1, f, row);
           tg[2][3] = P(k - 1, f, row);
         }
-        visc_flux(P(k, f - 1, row), P(k, f, row), tg, 0, dr, mu, kq, IDIM, G);
+        visc_flux<EX>(P(k, f - 1, row), P(k, f, row), tg, 0, dr, idr, mu, kq, IDIM, G);
       } else {
         const int w2 = w - NXF, col = w2 % TX, f = w2 / TX;  // face between rows f-1 and f
         tg[0][0] = P(k, col + 1, f - 1);
@@ -333,7 +348,7 @@ __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* block
           tg[2][2] = P(k + 1, col, f);
           tg[2][3] = P(k - 1, col, f);
         }
-        visc_flux(P(k, col, f - 1), P(k, col, f), tg, 1, dr, mu, kq, IDIM, G);
+        visc_flux<EX>(P(k, col, f - 1), P(k, col, f), tg, 1, dr, idr, mu, kq, IDIM, G);
       }
 #pragma unroll
       for (int v = 0; v < 4; ++v) sg[v][w] = G[v + 1];
@@ -347,9 +362,14 @@ __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* block
       const int fxl = ty * (TX + 1) + tx, fyl = NXF + ty * TX + tx;
       double V[5] = {0, 0, 0, 0, 0};
       for (int v = 1; v < 5; ++v) {
-        V[v] = V[v] + (sg[v - 1][fxl + 1] - sg[v - 1][fxl]) / dr[0];
-        V[v] = V[v] + (sg[v - 1][fyl + TX] - sg[v - 1][fyl]) / dr[1];
-        if (IDIM == 3) V[v] = V[v] + (Gzr[v] - Gzl[v]) / dr[2];
+        if constexpr (EX) {
+          V[v] = V[v] + (sg[v - 1][fxl + 1] - sg[v - 1][fxl]) / dr[0];
+          V[v] = V[v] + (sg[v - 1][fyl + TX] - sg[v - 1][fyl]) / dr[1];
+          if (IDIM == 3) V[v] = V[v] + (Gzr[v] - Gzl[v]) / dr[2];
+        } else {
+          V[v] = (sg[v - 1][fxl + 1] - sg[v - 1][fxl]) * idr[0] + (sg[v - 1][fyl + TX] - sg[v - 1][fyl]) * idr[1];
+          if (IDIM == 3) V[v] = V[v] + (Gzr[v] - Gzl[v]) * idr[2];
+        }
       }
       V[0] = 0.0 + (0.0 - 0.0) / dr[0];
       const int64_t o = (T.x0 + tx) + (int64_t)(T.y0 + ty) * B.sy + (int64_t)k * B.sz;
@@ -358,6 +378,21 @@ __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* block
 #pragma unroll
     for (int v = 0; v < 5; ++v) Gzl[v] = Gzr[v];
   }
+}
+
+template <int TX, int TY, int IDIM>
+__global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* blocks, const DevCase* cases,
+                                                          const Task* tasks, int role) {
+  constexpr int NR = IDIM == 3 ? 3 : 1;
+  __shared__ VPrim sp[NR][(TX + 2) * (TY + 2)];
+  __shared__ double sg[4][(TX + 1) * TY + TX * (TY + 1)];
+  const Task T = tasks[blockIdx.x];
+  const DevBlock& B = blocks[T.blk];
+  const DevCase& C = cases[B.case_id];
+  if (C.precision == PREC_EXACT)
+    visc_tile_body<TX, TY, IDIM, true>(B, C, T, role, sp, sg);
+  else
+    visc_tile_body<TX, TY, IDIM, false>(B, C, T, role, sp, sg);
 }
 
 // ---------------------------------------------------------------- launchers

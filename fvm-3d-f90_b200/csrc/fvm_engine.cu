@@ -886,6 +886,7 @@ int Engine::plan() {
     d.rk_stages = c.rk_stages;
     d.equation = c.equation;
     d.store_rhs = c.store_rhs;
+    d.precision = c.precision;
     d.block0 = (int)case_blk.size();
     d.nblocks = 0;
     if (cases[ci].dead) continue;

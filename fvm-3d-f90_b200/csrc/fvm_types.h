@@ -53,7 +53,7 @@ struct DevCase {
   int32_t block0;              // first entry of the case in the case-block index list
   int32_t equation;
   int32_t store_rhs;
-  int32_t pad_;
+  int32_t precision;           // fvm_precision of the case
 };
 
 // Per-case evolving scalars, written only by the finalize kernel.

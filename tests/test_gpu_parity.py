@@ -112,6 +112,15 @@ def test_navier_stokes_tgv_exact():
     np.testing.assert_allclose(rag, rao, rtol=1e-12)
 
 
+def test_navier_stokes_fast_fp64_1e12():
+    # the FP64 form's viscous terms multiply by reciprocal cell sizes instead
+    # of dividing: within 1e-12 of the oracle's exact form on the smooth TGV
+    c = cases.taylor_green(N=16)
+    g, o, _, _ = run_both(c, 3, gpu_over=dict(precision=abi.PREC_FP64))
+    a, r = g.get_state(0), o.get_state(0)
+    assert np.abs(a - r).max() <= 1e-12 * np.abs(r).max()
+
+
 def test_navier_stokes_blocks_exact():
     # 8 uneven periodic blocks: connected faces and the layer-1 edge ghosts of
     # the viscous stencil, partial viscous tiles
