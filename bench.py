@@ -377,8 +377,11 @@ def tgv(args):
         s = c.apply(Solver(c.config(precision=prec)))
         s.step(1)
         ms = tuning.time_step(s, steps)
+        prof = tuning.profile_step(s)
         ke[name] = cases.kinetic_energy(s.get_state(0), dV)
-        out[name] = {"ms_per_step": ms, "value": c.ncells * 3 / (ms * 1e-3) / 1e9}
+        out[name] = {"ms_per_step": ms, "value": c.ncells * 3 / (ms * 1e-3) / 1e9,
+                     "profile_ms": {k: round(sum(t for kk, t in prof if kk == k), 4)
+                                    for k in ("stage", "viscous", "gather", "finalize")}}
         s.close()
     out["ke_rel_diff_fp32_vs_fp64"] = abs(ke["fp32_flux"] - ke["fp64"]) / ke["fp64"]
     out["unit"] = UNIT
