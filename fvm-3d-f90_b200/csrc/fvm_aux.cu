@@ -186,8 +186,11 @@ __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, co
 // Central second-order viscous contribution (the reference's
 // viscous_flux_sub, class_space_discret.f90:671-675, is empty; this is the
 // textbook form): V = (dGx + dGy) + dGz with dG = (G(i+1/2) - G(i-1/2)) / dr.
-struct VPrim {
-  double u, v, w, th;
+// Cell primitives the viscous stencil reads, in the arithmetic type R of the
+// case's precision form (FP64, or FP32 for the FP32 flux form).
+template <class R>
+struct VPrimT {
+  R u, v, w, th;
 };
 
 __device__ __forceinline__ int64_t vcell(const DevBlock& B, int x, int y, int z) {
@@ -201,10 +204,11 @@ __device__ __forceinline__ int64_t vcell(const DevBlock& B, int x, int y, int z)
   return x + (int64_t)y * B.sy + (int64_t)z * B.sz;
 }
 
-// EX: the exact expression trees (divisions); otherwise one reciprocal.
-template <bool EX>
-__device__ __forceinline__ VPrim vprim(const double* q, int64_t o, int64_t vs, double gm1) {
-  VPrim r;
+// EX: the exact expression trees (divisions); otherwise one reciprocal (in
+// FP64, stored in R).
+template <bool EX, class R>
+__device__ __forceinline__ VPrimT<R> vprim(const double* q, int64_t o, int64_t vs, double gm1) {
+  VPrimT<R> r;
   if constexpr (EX) {
     Prim5<double> p = cons2prim<double, true>(q[o], q[o + vs], q[o + 2 * vs], q[o + 3 * vs], q[o + 4 * vs], gm1);
     r.u = p.u;
@@ -214,15 +218,17 @@ __device__ __forceinline__ VPrim vprim(const double* q, int64_t o, int64_t vs, d
   } else {
     const double q0 = q[o], q1 = q[o + vs], q2 = q[o + 2 * vs], q3 = q[o + 3 * vs], q4 = q[o + 4 * vs];
     const double ir = 1.0 / q0;
-    r.u = q1 * ir;
-    r.v = q2 * ir;
-    r.w = q3 * ir;
-    r.th = gm1 * (q4 - 0.5 * (q1 * r.u + q2 * r.v + q3 * r.w)) * ir;
+    const double u = q1 * ir, v = q2 * ir, w = q3 * ir;
+    r.u = (R)u;
+    r.v = (R)v;
+    r.w = (R)w;
+    r.th = (R)(gm1 * (q4 - 0.5 * (q1 * u + q2 * v + q3 * w)) * ir);
   }
   return r;
 }
 
-__device__ __forceinline__ double vcomp(const VPrim& p, int m) {
+template <class R>
+__device__ __forceinline__ R vcomp(const VPrimT<R>& p, int m) {
   return m == 0 ? p.u : (m == 1 ? p.v : (m == 2 ? p.w : p.th));
 }
 
@@ -231,34 +237,33 @@ __device__ __forceinline__ double vcomp(const VPrim& p, int m) {
 // L + e_d, L - e_d, R + e_d, R - e_d; the tangential gradient is the mean of
 // the two central differences.
 // EX divides by the cell sizes; otherwise multiplies by their reciprocals.
-template <bool EX>
-__device__ __forceinline__ void visc_flux(const VPrim& L, const VPrim& R, const VPrim (*tg)[4], int dir,
-                                          const double dr[3], const double idr[3], double mu, double kq, int idim,
-                                          double G[5]) {
-  double grad[4][3];
+template <bool EX, class T>
+__device__ __forceinline__ void visc_flux(const VPrimT<T>& L, const VPrimT<T>& R, const VPrimT<T> (*tg)[4], int dir,
+                                          const T dr[3], const T idr[3], T mu, T kq, int idim, T G[5]) {
+  T grad[4][3];
   for (int m = 0; m < 4; ++m)
-    for (int d = 0; d < 3; ++d) grad[m][d] = 0.0;
+    for (int d = 0; d < 3; ++d) grad[m][d] = T(0);
   for (int m = 0; m < 4; ++m)
     grad[m][dir] = EX ? (vcomp(R, m) - vcomp(L, m)) / dr[dir] : (vcomp(R, m) - vcomp(L, m)) * idr[dir];
   for (int d = 0; d < idim; ++d) {
     if (d == dir) continue;
-    const VPrim& lp = tg[d][0];
-    const VPrim& lm = tg[d][1];
-    const VPrim& rp = tg[d][2];
-    const VPrim& rm = tg[d][3];
+    const VPrimT<T>& lp = tg[d][0];
+    const VPrimT<T>& lm = tg[d][1];
+    const VPrimT<T>& rp = tg[d][2];
+    const VPrimT<T>& rm = tg[d][3];
     for (int m = 0; m < 4; ++m) {
-      const double s = (vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m));
-      grad[m][d] = EX ? s / (4.0 * dr[d]) : s * (0.25 * idr[d]);
+      const T s = (vcomp(lp, m) - vcomp(lm, m)) + (vcomp(rp, m) - vcomp(rm, m));
+      grad[m][d] = EX ? s / (T(4.0) * dr[d]) : s * (T(0.25) * idr[d]);
     }
   }
-  const double div = grad[0][0] + grad[1][1] + grad[2][2];
-  const double uf[3] = {0.5 * (L.u + R.u), 0.5 * (L.v + R.v), 0.5 * (L.w + R.w)};
-  double tau[3];
+  const T div = grad[0][0] + grad[1][1] + grad[2][2];
+  const T uf[3] = {T(0.5) * (L.u + R.u), T(0.5) * (L.v + R.v), T(0.5) * (L.w + R.w)};
+  T tau[3];
   for (int m = 0; m < 3; ++m) {
     tau[m] = mu * (grad[m][dir] + grad[dir][m]);
-    if (m == dir) tau[m] = tau[m] - 2.0 / 3.0 * mu * div;
+    if (m == dir) tau[m] = tau[m] - T(2.0 / 3.0) * mu * div;
   }
-  G[0] = 0.0;
+  G[0] = T(0);
   G[1] = tau[0];
   G[2] = tau[1];
   G[3] = tau[2];
@@ -272,18 +277,22 @@ __device__ __forceinline__ void visc_flux(const VPrim& L, const VPrim& R, const 
 // one carried in registers). V = (dGx + dGy) + dGz as in the per-cell form.
 // EX: the exact form the exact-FP64 cases need for parity with the oracle;
 // the other precision forms multiply by reciprocals instead of dividing.
-template <int TX, int TY, int IDIM, bool EX>
+template <int TX, int TY, int IDIM, bool EX, class R>
 __device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase& C, const Task& T, int role,
-                                               VPrim (*sp)[(TX + 2) * (TY + 2)],
-                                               double (*sg)[(TX + 1) * TY + TX * (TY + 1)]) {
+                                               unsigned char* smem) {
+  using VPrim = VPrimT<R>;
   constexpr int NT = TX * TY, PX = TX + 2;
   constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1), NF = NXF + NYF;
   constexpr int PL = (TX + 2) * (TY + 2);
+  constexpr int NR = IDIM == 3 ? 3 : 1;
+  VPrim (*sp)[PL] = reinterpret_cast<VPrim (*)[PL]>(smem);
+  R (*sg)[NF] = reinterpret_cast<R (*)[NF]>(smem + sizeof(VPrim) * NR * PL);
   const double* q = B.q[role];
   const int64_t vs = B.vs;
-  const double gm1 = C.gm1, mu = C.mu, kq = C.kq;
-  const double dr[3] = {B.dr[0], B.dr[1], B.dr[2]};
-  const double idr[3] = {B.inv_dr[0], B.inv_dr[1], B.inv_dr[2]};
+  const double gm1 = C.gm1;
+  const R mu = (R)C.mu, kq = (R)C.kq;
+  const R dr[3] = {(R)B.dr[0], (R)B.dr[1], (R)B.dr[2]};
+  const R idr[3] = {(R)B.inv_dr[0], (R)B.inv_dr[1], (R)B.inv_dr[2]};
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const bool act = (T.x0 + tx < B.n[0]) && (T.y0 + ty < B.n[1]);
   auto slot = [](int z) { return IDIM == 3 ? ((z % 3) + 3) % 3 : 0; };
@@ -294,12 +303,12 @@ __device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase&
     for (int w = tid; w < PL; w += NT) {
       const int x = min(max(T.x0 + w % PX - 1, -1), B.n[0]);
       const int y = min(max(T.y0 + w / PX - 1, -1), B.n[1]);
-      dst[w] = vprim<EX>(q, vcell(B, x, y, z), vs, gm1);
+      dst[w] = vprim<EX, R>(q, vcell(B, x, y, z), vs, gm1);
     }
   };
   auto P = [&](int z, int x, int y) -> const VPrim& { return sp[slot(z)][(y + 1) * PX + (x + 1)]; };
   // z face between planes z and z+1 of this thread's column
-  auto zface = [&](int z, double G[5]) {
+  auto zface = [&](int z, R G[5]) {
     VPrim tg[3][4];
     tg[0][0] = P(z, tx + 1, ty);
     tg[0][1] = P(z, tx - 1, ty);
@@ -312,7 +321,7 @@ __device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase&
     visc_flux<EX>(P(z, tx, ty), P(z + 1, tx, ty), tg, 2, dr, idr, mu, kq, 3, G);
   };
 
-  double Gzl[5] = {0, 0, 0, 0, 0}, Gzr[5] = {0, 0, 0, 0, 0};
+  R Gzl[5] = {0, 0, 0, 0, 0}, Gzr[5] = {0, 0, 0, 0, 0};
   if (IDIM == 3) {
     fill(T.z0 - 1);
     fill(T.z0);
@@ -322,7 +331,7 @@ __device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase&
     __syncthreads();
     for (int w = tid; w < NF; w += NT) {
       VPrim tg[3][4];
-      double G[5];
+      R G[5];
       if (w < NXF) {
         const int f = w % (TX + 1), row = w / (TX + 1);  // face between cells f-1 and f
         tg[1][0] = P(k, f - 1, row + 1);
@@ -360,7 +369,7 @@ __device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase&
     __syncthreads();
     if (act) {
       const int fxl = ty * (TX + 1) + tx, fyl = NXF + ty * TX + tx;
-      double V[5] = {0, 0, 0, 0, 0};
+      R V[5] = {0, 0, 0, 0, 0};
       for (int v = 1; v < 5; ++v) {
         if constexpr (EX) {
           V[v] = V[v] + (sg[v - 1][fxl + 1] - sg[v - 1][fxl]) / dr[0];
@@ -371,9 +380,9 @@ __device__ __forceinline__ void visc_tile_body(const DevBlock& B, const DevCase&
           if (IDIM == 3) V[v] = V[v] + (Gzr[v] - Gzl[v]) * idr[2];
         }
       }
-      V[0] = 0.0 + (0.0 - 0.0) / dr[0];
+      V[0] = R(0);
       const int64_t o = (T.x0 + tx) + (int64_t)(T.y0 + ty) * B.sy + (int64_t)k * B.sz;
-      for (int v = 0; v < 5; ++v) B.visc[o + v * vs] = V[v];
+      for (int v = 0; v < 5; ++v) B.visc[o + v * vs] = (double)V[v];
     }
 #pragma unroll
     for (int v = 0; v < 5; ++v) Gzl[v] = Gzr[v];
@@ -384,15 +393,18 @@ template <int TX, int TY, int IDIM>
 __global__ void __launch_bounds__(TX* TY) visc_tile_kernel(const DevBlock* blocks, const DevCase* cases,
                                                           const Task* tasks, int role) {
   constexpr int NR = IDIM == 3 ? 3 : 1;
-  __shared__ VPrim sp[NR][(TX + 2) * (TY + 2)];
-  __shared__ double sg[4][(TX + 1) * TY + TX * (TY + 1)];
+  // storage of the FP64 forms; the FP32 form uses the first half
+  __shared__ __align__(16) unsigned char smem[sizeof(VPrimT<double>) * NR * (TX + 2) * (TY + 2) +
+                                              sizeof(double) * 4 * ((TX + 1) * TY + TX * (TY + 1))];
   const Task T = tasks[blockIdx.x];
   const DevBlock& B = blocks[T.blk];
   const DevCase& C = cases[B.case_id];
   if (C.precision == PREC_EXACT)
-    visc_tile_body<TX, TY, IDIM, true>(B, C, T, role, sp, sg);
+    visc_tile_body<TX, TY, IDIM, true, double>(B, C, T, role, smem);
+  else if (C.precision == PREC_FP32)
+    visc_tile_body<TX, TY, IDIM, false, float>(B, C, T, role, smem);
   else
-    visc_tile_body<TX, TY, IDIM, false>(B, C, T, role, sp, sg);
+    visc_tile_body<TX, TY, IDIM, false, double>(B, C, T, role, smem);
 }
 
 // ---------------------------------------------------------------- launchers

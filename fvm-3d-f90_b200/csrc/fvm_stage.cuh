@@ -44,18 +44,21 @@ struct StageCfg {
   // face items
   static constexpr int NT = (NC + 127) / 128 * 128;
   static constexpr int PW = TX + 2 * H, PH = TY + 2 * H;
-  static constexpr int NODEV = RECON == RECON_WENO_ ? (TB ? 10 : 5) : 0;
+  // node values per x / y node item: WENO 5 (left-biased) or 10 (both
+  // sides); MUSCL 10 (the cell's values at its right and left faces)
+  static constexpr int NODEV = RECON == RECON_WENO_ ? (TB ? 10 : 5) : (RECON == RECON_MUSCL_ ? 10 : 0);
   static constexpr int NXN = (TX + 2) * TY, NYN = TX * (TY + 2);
   static constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);
   static constexpr int NW = 2 * H * (TX + TY);             // halo cells of a plane
   static constexpr int NPL = (DIM == 2 ? NC : 0) + NW;     // plane cells loaded from HBM
   static constexpr int NPS = (NPL + NT - 1) / NT;          // per-thread load slots
   static constexpr int WIN = H + 2;                        // z window: planes k-1 .. k+H
-  static constexpr int WZ = RECON == RECON_WENO_ ? 2 : 1;  // warm-up planes before z0
+  static constexpr int WZ = RECON == RECON_SIMPLE_ ? 1 : 2;  // warm-up planes before z0
   // R arrays first, then the FP64 staging of the cell's q0 / q_in / acc
-  // WENO reads the plane only in phase A, so the face fluxes (phase B / C)
-  // share its storage; a barrier then separates phase C from the refill
-  static constexpr bool FAL = RECON == RECON_WENO_;
+  // WENO and MUSCL read the plane only in phase A (their face states are
+  // node values), so the face fluxes (phase B / C) share its storage; a
+  // barrier then separates phase C from the refill
+  static constexpr bool FAL = RECON != RECON_SIMPLE_;
   static constexpr size_t PF = FAL ? (5 * PH * PW > 5 * (NXF + NYF) ? 5 * PH * PW : 5 * (NXF + NYF))
                                    : 5 * PH * PW + 5 * (NXF + NYF);
   static constexpr size_t r_elems = (size_t)(PF + NODEV * (NXN + NYN));
@@ -680,27 +683,78 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         }
       }
 
+      if constexpr (RECON == RECON_MUSCL_) {
+        // MUSCL node of a cell: its values at its right face (qR, the left
+        // state of that face) and at its left face (qL), one limited slope
+        // pair per cell (scheme_reconstruct_MUSCL.f90:114-226); TEXTBOOK
+        // falls back to the cell value where a state is not admissible
+        auto node = [&](const R (&p)[5][3], R (&qr)[5], R (&ql)[5]) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            R Dbm, Dbp;
+            muscl_slopes(p[v][0], p[v][1], p[v][2], K.limiter, Dbm, Dbp);
+            qr[v] = p[v][1] + R(0.25) * (K.omk * Dbm + K.opk * Dbp);
+            ql[v] = p[v][1] - R(0.25) * (K.omk * Dbp + K.opk * Dbm);
+          }
+          if (K.textbook) {
+            if (!admissible(mkprim(qr)))
+#pragma unroll
+              for (int v = 0; v < 5; ++v) qr[v] = p[v][1];
+            if (!admissible(mkprim(ql)))
+#pragma unroll
+              for (int v = 0; v < 5; ++v) ql[v] = p[v][1];
+          }
+        };
+        if (DIM == 3 && colt) {
+          // node of plane k+1 from planes k .. k+2 (window slots 1..3)
+          R p[5][3], qr[5], ql[5];
+#pragma unroll
+          for (int v = 0; v < 5; ++v)
+#pragma unroll
+            for (int s = 0; s < 3; ++s) p[v][s] = zw[s + 1][v];
+          node(p, qr, ql);
+          zWm_cur = mkprim(qr);  // left state of face k+3/2, carried
+          zWcur = mkprim(ql);    // right state of face k+1/2
+        }
+        if (do_xy) {
+          constexpr int NN = C::NXN + C::NYN;
+          for (int w = tid; w < NN; w += NT) {
+            R p[5][3], qr[5], ql[5];
+            if (w < C::NXN) {
+              const int c = w % (TX + 2) - 1, row = w / (TX + 2);
+              const int base = (H + row) * PW + (H + c);
+#pragma unroll
+              for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int s = 0; s < 3; ++s) p[v][s] = sP[v * PLANE + base + s - 1];
+            } else {
+              const int w2 = w - C::NXN;
+              const int col = w2 % TX, c = w2 / TX - 1;
+              const int base = (H + c) * PW + (H + col);
+#pragma unroll
+              for (int v = 0; v < 5; ++v)
+#pragma unroll
+                for (int s = 0; s < 3; ++s) p[v][s] = sP[v * PLANE + base + (s - 1) * PW];
+            }
+            node(p, qr, ql);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              sN[v * NN + w] = qr[v];
+              sN[(5 + v) * NN + w] = ql[v];
+            }
+          }
+          __syncthreads();
+        }
+      }
+
       // ---- phase B: fluxes ---------------------------------------------------
       R zF[5] = {0, 0, 0, 0, 0};
       if constexpr (DIM == 3) {
         if (colt && k >= T.z0 - 1) {
           Prim5<R> L, Rr;
-          if constexpr (RECON == RECON_WENO_) {
+          if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
             L = zWprev;
             Rr = zWcur;
-          } else if constexpr (RECON == RECON_MUSCL_) {
-            R l[5], r[5];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-              l[v] = muscl_left(zw[0][v], zw[1][v], zw[2][v], K);
-              r[v] = muscl_right(zw[1][v], zw[2][v], zw[3][v], K);
-            }
-            L = mkprim(l);
-            Rr = mkprim(r);
-            if (K.textbook) {
-              if (!admissible(L)) L = mkprim(zw[1]);
-              if (!admissible(Rr)) Rr = mkprim(zw[2]);
-            }
           } else {
             L = mkprim(zw[1]);
             Rr = mkprim(zw[2]);
@@ -716,11 +770,11 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
           if (w < C::NXF) {
             const int f = w % (TX + 1), row = w / (TX + 1);
             Prim5<R> L, Rr;
-            if constexpr (RECON == RECON_WENO_) {
+            if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
               const int nl = row * (TX + 2) + f, nr = nl + 1;
               L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
               L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
-              const int o = TB ? 5 : 0;
+              const int o = (TB || RECON == RECON_MUSCL_) ? 5 : 0;
               Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
               Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
             } else {
@@ -728,38 +782,22 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
               R l[5], r[5];
 #pragma unroll
               for (int v = 0; v < 5; ++v) {
-                const R* pv = sP + v * PLANE + base;
-                if constexpr (RECON == RECON_MUSCL_) {
-                  l[v] = muscl_left(pv[-2], pv[-1], pv[0], K);
-                  r[v] = muscl_right(pv[-1], pv[0], pv[1], K);
-                } else {
-                  l[v] = pv[-1];
-                  r[v] = pv[0];
-                }
+                l[v] = sP[v * PLANE + base - 1];
+                r[v] = sP[v * PLANE + base];
               }
               L = mkprim(l);
               Rr = mkprim(r);
-              if (RECON == RECON_MUSCL_ && K.textbook && !(admissible(L) && admissible(Rr))) {
-                R c0[5], c1[5];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                  c0[v] = sP[v * PLANE + base - 1];
-                  c1[v] = sP[v * PLANE + base];
-                }
-                if (!admissible(L)) L = mkprim(c0);
-                if (!admissible(Rr)) Rr = mkprim(c1);
-              }
             }
             face_flux<FLUX, 0, R, EX>(L, Rr, K, F);
           } else {
             const int w2 = w - C::NXF;
             const int col = w2 % TX, f = w2 / TX;
             Prim5<R> L, Rr;
-            if constexpr (RECON == RECON_WENO_) {
+            if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
               const int nl = C::NXN + f * TX + col, nr = nl + TX;
               L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
               L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
-              const int o = TB ? 5 : 0;
+              const int o = (TB || RECON == RECON_MUSCL_) ? 5 : 0;
               Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
               Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
             } else {
@@ -767,27 +805,11 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
               R l[5], r[5];
 #pragma unroll
               for (int v = 0; v < 5; ++v) {
-                const R* pv = sP + v * PLANE + base;
-                if constexpr (RECON == RECON_MUSCL_) {
-                  l[v] = muscl_left(pv[-2 * PW], pv[-PW], pv[0], K);
-                  r[v] = muscl_right(pv[-PW], pv[0], pv[PW], K);
-                } else {
-                  l[v] = pv[-PW];
-                  r[v] = pv[0];
-                }
+                l[v] = sP[v * PLANE + base - PW];
+                r[v] = sP[v * PLANE + base];
               }
               L = mkprim(l);
               Rr = mkprim(r);
-              if (RECON == RECON_MUSCL_ && K.textbook && !(admissible(L) && admissible(Rr))) {
-                R c0[5], c1[5];
-#pragma unroll
-                for (int v = 0; v < 5; ++v) {
-                  c0[v] = sP[v * PLANE + base - PW];
-                  c1[v] = sP[v * PLANE + base];
-                }
-                if (!admissible(L)) L = mkprim(c0);
-                if (!admissible(Rr)) Rr = mkprim(c1);
-              }
             }
             face_flux<FLUX, 1, R, EX>(L, Rr, K, F);
           }
@@ -917,7 +939,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       if (DIM == 3 && colt) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) zFprev[v] = zF[v];
-        if constexpr (RECON == RECON_WENO_) zWprev = zWm_cur;
+        if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) zWprev = zWm_cur;
 #pragma unroll
         for (int s = 0; s + 1 < C::WIN; ++s)
 #pragma unroll
