@@ -17,12 +17,18 @@ cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* c
                            unsigned long long* case_max, int role, cudaStream_t s);
 cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                             int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s);
-// Viscous contribution of the Navier-Stokes blocks: one CTA per task of the
+// Viscous contribution of the Navier-Stokes blocks: one CTA per task of a
 // viscous task list (kViscTX x kViscTY column tiles over z ranges), all of
-// dimension idim.
-constexpr int kViscTX = 16, kViscTY = 8, kViscZ = 16;
+// dimension idim and precision form prec (PREC_*). visc_occupancy: CTAs of
+// the 3D kernel of that form resident on one SM. The *_fast entry points
+// serve the FP64 and FP32 forms.
+constexpr int kViscTX = 16, kViscTY = 8;
 cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
-                        int role, cudaStream_t s);
+                        int prec, int role, cudaStream_t s);
+cudaError_t visc_occupancy(int prec, int* ctas_per_sm);
+cudaError_t launch_visc_fast(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
+                             int prec, int role, cudaStream_t s);
+cudaError_t visc_occupancy_fast(int prec, int* ctas_per_sm);
 
 // One compiled instantiation of the fused stage kernel.
 struct StageKernelInfo {

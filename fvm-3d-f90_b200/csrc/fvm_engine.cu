@@ -764,34 +764,71 @@ int Engine::plan() {
   }
   ntasks_total = (int64_t)tasks.size();
 
-  // -- viscous task list: Navier-Stokes blocks in column tiles over equal z
-  // chunks, 3D blocks first, then 2D
-  vtask_off_ = (int)tasks.size();
-  for (int dim : {3, 2}) {
-    const int before = (int)tasks.size();
-    std::vector<int64_t> z0s;
-    for (int bi : live_blocks) {
-      const HBlock& b = blocks[bi];
-      const fvm_config& c = cases[b.case_id].cfg;
-      if (c.equation != FVM_EQ_NAVIER_STOKES || c.idimension != dim) continue;
-      if (dim == 3)
-        equal_chunks(b.n[2], kViscZ, z0s);
-      else
-        z0s = {0, b.n[2]};
-      for (size_t ch = 0; ch + 1 < z0s.size(); ++ch)
-        for (int64_t y0 = 0; y0 < b.n[1]; y0 += kViscTY)
-          for (int64_t x0 = 0; x0 < b.n[0]; x0 += kViscTX) {
-            Task t;
-            t.blk = bi;
-            t.x0 = (int)x0;
-            t.y0 = (int)y0;
-            t.z0 = (int)z0s[ch];
-            t.z1 = (int)z0s[ch + 1];
-            t.slot = 0;
-            tasks.push_back(t);
+  // -- viscous task lists, one per (precision form, dimension): Navier-Stokes
+  // blocks in column tiles over equal z chunks. The kernel is
+  // throughput-bound per SM (its CTAs share the SM's shared-memory pipe), so
+  // a 3D chunk length is scored by the largest per-SM sum of task costs
+  // (longest-first onto the SMs) over the CTAs an SM holds, but no less than
+  // half the longest task (an SM left with one task runs it at most about
+  // twice as fast). A task of c planes costs c plane-times plus its prologue
+  // (two extra planes converted, one extra z face).
+  for (int prec = 0; prec < 3; ++prec) {
+    for (int dim : {3, 2}) {
+      const int li = prec * 2 + (dim == 3 ? 0 : 1);
+      vlist_off_[li] = (int)tasks.size();
+      std::vector<const HBlock*> ns;
+      for (int bi : live_blocks) {
+        const fvm_config& c = cases[blocks[bi].case_id].cfg;
+        if (c.equation == FVM_EQ_NAVIER_STOKES && c.idimension == dim && c.precision == prec)
+          ns.push_back(&blocks[bi]);
+      }
+      int64_t vz = 16;
+      std::vector<int64_t> z0s;
+      if (dim == 3 && !ns.empty()) {
+        int occ = 1;
+        CK(visc_occupancy(prec, &occ));
+        double best = 0.0;
+        std::vector<double> cost;
+        for (int64_t cand = 64; cand >= 4; cand -= (cand > 16 ? 4 : 2)) {
+          cost.clear();
+          double longest = 0.0;
+          for (const HBlock* b : ns) {
+            const int64_t ncol = ((b->n[0] + kViscTX - 1) / kViscTX) * ((b->n[1] + kViscTY - 1) / kViscTY);
+            equal_chunks(b->n[2], cand, z0s);
+            for (size_t c = 0; c + 1 < z0s.size(); ++c)
+              for (int64_t q = 0; q < ncol; ++q) {
+                cost.push_back((double)(z0s[c + 1] - z0s[c]) + 1.5);
+                longest = std::max(longest, cost.back());
+              }
           }
+          const double m = std::max(queue_makespan(cost, num_sms) / occ, 0.5 * longest);
+          if (best <= 0.0 || m < best * 0.995) {
+            best = m;
+            vz = cand;
+          }
+        }
+      }
+      for (const HBlock* b : ns) {
+        const int bi = (int)(b - blocks.data());
+        if (dim == 3)
+          equal_chunks(b->n[2], vz, z0s);
+        else
+          z0s = {0, b->n[2]};
+        for (size_t ch = 0; ch + 1 < z0s.size(); ++ch)
+          for (int64_t y0 = 0; y0 < b->n[1]; y0 += kViscTY)
+            for (int64_t x0 = 0; x0 < b->n[0]; x0 += kViscTX) {
+              Task t;
+              t.blk = bi;
+              t.x0 = (int)x0;
+              t.y0 = (int)y0;
+              t.z0 = (int)z0s[ch];
+              t.z1 = (int)z0s[ch + 1];
+              t.slot = 0;
+              tasks.push_back(t);
+            }
+      }
+      vlist_n_[li] = (int)tasks.size() - vlist_off_[li];
     }
-    (dim == 3 ? nvtask3_ : nvtask2_) = (int)tasks.size() - before;
   }
 
   // -- ghost gather pairs (slab element offsets)
@@ -1009,12 +1046,10 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
   for (int m = 1; m <= S; ++m) {
     int rin, rout;
     stage_roles(S, m, &rin, &rout);
-    if (nvtask3_ > 0) {
-      CK(launch_visc(d_blocks_, d_cases_, d_tasks_ + vtask_off_, nvtask3_, 3, rin, stream));
-      CK(mark(3));
-    }
-    if (nvtask2_ > 0) {
-      CK(launch_visc(d_blocks_, d_cases_, d_tasks_ + vtask_off_ + nvtask3_, nvtask2_, 2, rin, stream));
+    for (int li = 0; li < 6; ++li) {
+      if (vlist_n_[li] == 0) continue;
+      CK(launch_visc(d_blocks_, d_cases_, d_tasks_ + vlist_off_[li], vlist_n_[li], li % 2 == 0 ? 3 : 2, li / 2,
+                     rin, stream));
       CK(mark(3));
     }
     if (fork) CK(cudaEventRecord(fork_ev_[ev_i], stream));

@@ -159,7 +159,8 @@ class Engine {
   int64_t* d_pairs_ = nullptr;
   int* d_counters_ = nullptr;
   int ncounters_ = 0;
-  int vtask_off_ = 0, nvtask3_ = 0, nvtask2_ = 0;  // viscous tasks in d_tasks_
+  // viscous task lists in d_tasks_, index precision * 2 + (3D ? 0 : 1)
+  int vlist_off_[6] = {0, 0, 0, 0, 0, 0}, vlist_n_[6] = {0, 0, 0, 0, 0, 0};
   std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..C][plane, z] (null: no TMA)
   int32_t* d_err_ = nullptr;          // kernel error flag (a tensor copy that did not arrive)
   bool drop_copies_ = false;          // test hook: tensor copies armed but not issued
