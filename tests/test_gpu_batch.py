@@ -120,3 +120,28 @@ def test_server_admission_cap():
     srv.close()
     assert stats["requests"] == 8 and stats["failed"] == 0
     assert max(seen) <= cap
+
+
+def test_navier_stokes_mixed_precisions_batched():
+    # one engine holding a Navier-Stokes case of each precision form (three
+    # viscous task lists, three viscous kernels) plus a 2D one: every case
+    # matches its own run alone bit for bit, the exact one also the oracle
+    forms = [abi.PREC_FP64_EXACT, abi.PREC_FP64, abi.PREC_FP32_FLUX]
+    cs = [cases.taylor_green(N=16 + 4 * i, precision=p) for i, p in enumerate(forms)]
+    cs.append(cases.riemann2d(n=27, seed=3, nk=2, dt=1e-3, equation=abi.EQ_NAVIER_STOKES, mu=5e-3))
+    s = Solver(cs[0].config())
+    s.remove_case(0)
+    ids = []
+    for c in cs:
+        cid = s.add_case(c.config())
+        c.apply(s, case_id=cid)
+        ids.append(list(c.block_ids))
+    s.step(3)
+    for c, bid in zip(cs, ids):
+        ref = alone(c, 3)
+        for b, g in enumerate(bid):
+            assert np.array_equal(s.get_state(g), ref[b])
+    o = cs[0].apply(orc.Oracle(cs[0].config()))
+    o.step(3)
+    assert np.array_equal(s.get_state(ids[0][0]), o.get_state(0))
+    s.close()

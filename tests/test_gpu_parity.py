@@ -121,6 +121,20 @@ def test_navier_stokes_fast_fp64_1e12():
     assert np.abs(a - r).max() <= 1e-12 * np.abs(r).max()
 
 
+def test_navier_stokes_fp32_flux_l1():
+    # FP32 flux form (FP32 reconstruction, flux and viscous terms, FP64
+    # state and RK): relative L1 error against the exact oracle after three
+    # steps of the TGV, per conserved variable (momenta relative to their sum)
+    c = cases.taylor_green(N=24)
+    g, o, _, _ = run_both(c, 3, gpu_over=dict(precision=abi.PREC_FP32_FLUX))
+    a, r = g.get_state(0), o.get_state(0)
+    d = np.abs(a - r).reshape(5, -1).sum(axis=1)
+    mom = np.abs(r[1:4]).sum()
+    assert d[0] <= 1e-6 * np.abs(r[0]).sum()
+    assert d[4] <= 1e-6 * np.abs(r[4]).sum()
+    assert d[1:4].max() <= 1e-5 * mom
+
+
 def test_navier_stokes_blocks_exact():
     # 8 uneven periodic blocks: connected faces and the layer-1 edge ghosts of
     # the viscous stencil, partial viscous tiles
