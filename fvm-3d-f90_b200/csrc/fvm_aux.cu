@@ -233,6 +233,21 @@ cudaError_t visc_occupancy(int prec, int* ctas_per_sm) {
   return prec == PREC_EXACT ? visc_occupancy_prec<PREC_EXACT>(ctas_per_sm) : visc_occupancy_fast(prec, ctas_per_sm);
 }
 
+// The non-exact forms' FP64 reciprocal and reciprocal square root over an
+// array (a test hook: their error against the correctly rounded values).
+__global__ void fast_math_probe_kernel(const double* x, int64_t n, double* r, double* rs) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    r[i] = rcp_(x[i]);
+    rs[i] = rsqrt_(x[i]);
+  }
+}
+
+cudaError_t launch_fast_math_probe(const double* x, int64_t n, double* r, double* rs, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  fast_math_probe_kernel<<<grid_for(n, 256), 256, 0, s>>>(x, n, r, rs);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
                         int prec, int role, cudaStream_t s) {
   if (prec == PREC_EXACT) return launch_visc_prec<PREC_EXACT>(blocks, cases, tasks, ntasks, idim, role, s);

@@ -29,6 +29,8 @@ cudaError_t visc_occupancy(int prec, int* ctas_per_sm);
 cudaError_t launch_visc_fast(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
                              int prec, int role, cudaStream_t s);
 cudaError_t visc_occupancy_fast(int prec, int* ctas_per_sm);
+// rcp_ / rsqrt_ of the non-exact FP64 forms over x[0..n) (device arrays).
+cudaError_t launch_fast_math_probe(const double* x, int64_t n, double* r, double* rs, cudaStream_t s);
 
 // One compiled instantiation of the fused stage kernel.
 struct StageKernelInfo {

@@ -1515,6 +1515,20 @@ int fvm_test_drop_tensor_copies(fvm_ctx* ctx, int on) {
   return ctx->eng.set_drop_copies(on != 0);
 }
 
+int fvm_test_fast_math(const double* x, int64_t n, double* rcp_out, double* rsqrt_out) {
+  if (!x || !rcp_out || !rsqrt_out || n < 0) return FVM_ERR_INVALID;
+  if (n == 0) return FVM_OK;
+  const size_t bytes = sizeof(double) * (size_t)n;
+  double* d = nullptr;
+  if (cudaMalloc(&d, 3 * bytes) != cudaSuccess) return FVM_ERR_CUDA;
+  cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = fvm::launch_fast_math_probe(d, n, d + n, d + 2 * n, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(rcp_out, d + n, bytes, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(rsqrt_out, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? FVM_OK : FVM_ERR_CUDA;
+}
+
 int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n) {
   if (!ctx || !n) return FVM_ERR_INVALID;
   int rc = ctx->eng.ensure_planned();

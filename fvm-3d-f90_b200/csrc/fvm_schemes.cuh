@@ -35,12 +35,37 @@ template <class R> struct SchemeConst {
   int textbook;
 };
 
-__device__ __forceinline__ double rcp_(double x) { return 1.0 / x; }
+// rcp_ / rsqrt_ / nsqrt_ serve the non-exact forms only (the exact form
+// divides and takes IEEE square roots in the reference's order). In FP64
+// they start from the hardware approximation (rcp / rsqrt .approx.ftz.f64)
+// and take two Newton-Raphson steps, r <- r + r (1 - x r) and
+// y <- y + y (1 - x y^2) / 2, each of which squares the relative error, so
+// the result is within a couple of ulp of the correctly rounded one with no
+// special-case branch. Arguments are positive normal numbers (densities,
+// pressures, squared sound speeds, limiter and entropy-fix denominators);
+// a zero argument gives a non-finite result, as the exact division does.
+__device__ __forceinline__ double rcp_(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
 __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
 __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
-__device__ __forceinline__ double rsqrt_(double x) { return rsqrt(x); }
+__device__ __forceinline__ double rsqrt_(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-(x * y), y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-(x * y), y, 1.0);
+  return fma(0.5 * y, e, y);
+}
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double nsqrt_(double x) { return x * rsqrt_(x); }
+__device__ __forceinline__ float nsqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double abs_(double x) { return fabs(x); }
 __device__ __forceinline__ float abs_(float x) { return fabsf(x); }
 __device__ __forceinline__ double sgn1_(double x) { return copysign(1.0, x); }
@@ -75,7 +100,8 @@ __device__ __forceinline__ Prim5<R> cons2prim(R q0, R q1, R q2, R q3, R q4, R gm
 // ------------------------------------------------------------ MUSCL
 // scheme_reconstruct_MUSCL.f90:114-226. Limited differences of the centre
 // p2 of the stencil (p1, p2, p3).
-template <class R>
+// EX divides as the reference does; the other forms multiply by rcp_.
+template <class R, bool EX>
 __device__ __forceinline__ void muscl_slopes(R p1, R p2, R p3, int lim, R& Dbm, R& Dbp) {
   const R Dm = p2 - p1;
   const R Dp = p3 - p2;
@@ -84,29 +110,22 @@ __device__ __forceinline__ void muscl_slopes(R p1, R p2, R p3, int lim, R& Dbm, 
     Dbm = R(0.5) * (sgn1_(Dm) + sgn1_(Dp)) * min2_(abs_(Dm), abs_(Dp));
     Dbp = R(0.5) * (sgn1_(Dp) + sgn1_(Dm)) * min2_(abs_(Dp), abs_(Dm));
   } else if (lim == LIM_VANLEER_) {
-    Dbm = (sgn1_(Dm) + sgn1_(Dp)) * Dm * Dp / (abs_(Dm) + abs_(Dp) + R(1.0E-6));
+    if constexpr (EX)
+      Dbm = (sgn1_(Dm) + sgn1_(Dp)) * Dm * Dp / (abs_(Dm) + abs_(Dp) + R(1.0E-6));
+    else
+      Dbm = (sgn1_(Dm) + sgn1_(Dp)) * Dm * Dp * rcp_(abs_(Dm) + abs_(Dp) + R(1.0E-6));
     Dbp = Dbm;
   } else if (lim == LIM_VANALBADA_) {
-    Dbm = (Dm * (Dp * Dp + R(1.0E-6)) + Dp * (Dm * Dm + R(1.0E-6))) / (Dm * Dm + Dp * Dp + R(1.0E-6));
+    const R num = Dm * (Dp * Dp + R(1.0E-6)) + Dp * (Dm * Dm + R(1.0E-6));
+    if constexpr (EX)
+      Dbm = num / (Dm * Dm + Dp * Dp + R(1.0E-6));
+    else
+      Dbm = num * rcp_(Dm * Dm + Dp * Dp + R(1.0E-6));
     Dbp = Dbm;
   } else {  // none_ / NULL
     Dbm = Dm;
     Dbp = Dp;
   }
-}
-// wind = -1: left state of the face right of p2.
-template <class R>
-__device__ __forceinline__ R muscl_left(R p1, R p2, R p3, const SchemeConst<R>& k) {
-  R Dbm, Dbp;
-  muscl_slopes(p1, p2, p3, k.limiter, Dbm, Dbp);
-  return p2 + R(0.25) * (k.omk * Dbm + k.opk * Dbp);
-}
-// wind = +1: right state of the face left of p2.
-template <class R>
-__device__ __forceinline__ R muscl_right(R p1, R p2, R p3, const SchemeConst<R>& k) {
-  R Dbm, Dbp;
-  muscl_slopes(p1, p2, p3, k.limiter, Dbm, Dbp);
-  return p2 - R(0.25) * (k.omk * Dbp + k.opk * Dbm);
 }
 
 // ------------------------------------------------------------ WENO
@@ -230,8 +249,11 @@ __device__ __forceinline__ void weno5_node(const R (&u)[5][5], int textbook, R w
 
 // ------------------------------------------------------------ Roe
 // scheme_FDS_Roe.f90:25-177
-template <class R> __device__ __forceinline__ R entropy_fix_(R lam, R delta) {
-  return (lam > delta) ? lam : R(0.5) * (lam * lam + delta * delta) / delta;
+template <class R, bool EX> __device__ __forceinline__ R entropy_fix_(R lam, R delta) {
+  if constexpr (EX)
+    return (lam > delta) ? lam : R(0.5) * (lam * lam + delta * delta) / delta;
+  else
+    return (lam > delta) ? lam : R(0.5) * (lam * lam + delta * delta) * rcp_(delta);
 }
 
 template <int DIR, class R, bool EX>
@@ -251,7 +273,7 @@ __device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, 
   } else {
     H_l = k.goverg1 * L.p * rcp_(L.r) + R(0.5) * (L.u * L.u + L.v * L.v + L.w * L.w);
     H_r = k.goverg1 * Rs.p * rcp_(Rs.r) + R(0.5) * (Rs.u * Rs.u + Rs.v * Rs.v + Rs.w * Rs.w);
-    rho_b = sqrt_(L.r * Rs.r);
+    rho_b = nsqrt_(L.r * Rs.r);
     const R id = rcp_(L.r + rho_b);
     u_b = (L.r * L.u + rho_b * Rs.u) * id;
     v_b = (L.r * L.v + rho_b * Rs.v) * id;
@@ -272,9 +294,9 @@ __device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, 
     ic2 = rs * rs;
   }
   const R delta = k.fix * abs_(Vl_b + c_b);
-  const R lam1 = entropy_fix_(abs_(Vl_b - c_b), delta);
-  const R lam2 = entropy_fix_(abs_(Vl_b), delta);
-  const R lam5 = entropy_fix_(abs_(Vl_b + c_b), delta);
+  const R lam1 = entropy_fix_<R, EX>(abs_(Vl_b - c_b), delta);
+  const R lam2 = entropy_fix_<R, EX>(abs_(Vl_b), delta);
+  const R lam5 = entropy_fix_<R, EX>(abs_(Vl_b + c_b), delta);
   R d1_0, d234_0, d5_0;
   if constexpr (EX) {
     d1_0 = lam1 * (dp - rho_b * c_b * dVl) / (R(2.0) * c_b * c_b);

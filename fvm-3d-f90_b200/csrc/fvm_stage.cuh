@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 #pragma unroll
           for (int v = 0; v < 5; ++v) {
             R Dbm, Dbp;
-            muscl_slopes(p[v][0], p[v][1], p[v][2], K.limiter, Dbm, Dbp);
+            muscl_slopes<R, EX>(p[v][0], p[v][1], p[v][2], K.limiter, Dbm, Dbp);
             qr[v] = p[v][1] + R(0.25) * (K.omk * Dbm + K.opk * Dbp);
             ql[v] = p[v][1] - R(0.25) * (K.omk * Dbp + K.opk * Dbm);
           }

@@ -89,3 +89,28 @@ def test_error_paths():
     with pytest.raises(FvmError) as e:
         s.step(2)
     assert e.value.code == 4  # FVM_ERR_NONFINITE
+
+
+def test_fast_fp64_reciprocals_within_2ulp():
+    # the non-exact FP64 forms' reciprocal and reciprocal square root
+    # (hardware approximation + two Newton-Raphson steps) against correctly
+    # rounded references (long double), over normal arguments whose results
+    # are normal too
+    import ctypes
+
+    lib = abi.load_library()
+    lib.fvm_test_fast_math.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+    rng = np.random.default_rng(5)
+    x = np.concatenate([10.0 ** rng.uniform(-300, 300, 200_000), rng.uniform(0.5, 2.0, 200_000),
+                        np.nextafter(1.0, 2.0) + rng.uniform(0, 1e-12, 1000), 2.0 ** np.arange(-900, 901, 7),
+                        [1.0, 1.4, 0.4, 1e-6, 3.0, 7.0]])
+    r = np.empty_like(x)
+    rs = np.empty_like(x)
+    assert lib.fvm_test_fast_math(x.ctypes.data, x.size, r.ctypes.data, rs.ctypes.data) == 0
+    xl = x.astype(np.longdouble)
+    ref_r = (np.longdouble(1) / xl).astype(np.float64)
+    ref_rs = (np.longdouble(1) / np.sqrt(xl)).astype(np.float64)
+    ulp_r = np.abs(r - ref_r) / np.spacing(ref_r)
+    ulp_rs = np.abs(rs - ref_rs) / np.spacing(ref_rs)
+    assert ulp_r.max() <= 2.0, ulp_r.max()
+    assert ulp_rs.max() <= 2.0, ulp_rs.max()
