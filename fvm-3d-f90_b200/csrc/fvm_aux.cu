@@ -100,9 +100,9 @@ __global__ void wavespeed_kernel(const DevBlock* blocks, const DevCase* cases, i
 
 // dt of the first step: fix_timestep, or cfl / max wave-speed sum.
 __global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const unsigned long long* case_max,
-                               int ncases) {
+                               const int* mask, int ncases) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncases) return;
+  if (c >= ncases || !mask[c]) return;
   const DevCase& C = cases[c];
   st[c].dt = (C.timestep_set == 0) ? C.dt_fixed : C.cfl / __longlong_as_double((long long)case_max[c]);
 }
@@ -212,14 +212,14 @@ cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int 
 }
 
 cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* cases, DevCaseState* st, int ncases,
-                           unsigned long long* case_max, int role, cudaStream_t s) {
+                           unsigned long long* case_max, const int* mask, int role, cudaStream_t s) {
   cudaError_t e = cudaMemsetAsync(case_max, 0, sizeof(unsigned long long) * ncases, s);
   if (e != cudaSuccess) return e;
   if (nblocks > 0) {
     dim3 g(64, nblocks);
     wavespeed_kernel<<<g, 256, 0, s>>>(blocks, cases, role, case_max);
   }
-  init_dt_kernel<<<(ncases + 127) / 128, 128, 0, s>>>(cases, st, case_max, ncases);
+  init_dt_kernel<<<(ncases + 127) / 128, 128, 0, s>>>(cases, st, case_max, mask, ncases);
   return cudaGetLastError();
 }
 

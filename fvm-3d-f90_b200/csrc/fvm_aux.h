@@ -14,7 +14,7 @@ cudaError_t launch_unpack(double* role_blk, int64_t vs, int sy, int sz, int ni, 
 cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, double* dst,
                         int prim, double gm1, cudaStream_t s);
 cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* cases, DevCaseState* st, int ncases,
-                           unsigned long long* case_max, int role, cudaStream_t s);
+                           unsigned long long* case_max, const int* mask, int role, cudaStream_t s);
 cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                             int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s);
 // Viscous contribution of the Navier-Stokes blocks: one CTA per task of a

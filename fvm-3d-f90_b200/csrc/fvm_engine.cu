@@ -124,6 +124,9 @@ void Engine::release() {
   d_tmap_.clear();
   if (d_err_) cudaFree(d_err_);
   d_err_ = nullptr;
+  if (d_dtmask_) cudaFree(d_dtmask_);
+  d_dtmask_ = nullptr;
+  dtmask_cap_ = 0;
   for (auto& b : blocks) {
     if (b.rhs_dev) cudaFree(b.rhs_dev);
     b.rhs_dev = nullptr;
@@ -952,6 +955,7 @@ int Engine::plan() {
     CK(cudaMemcpyAsync(d_state_ + ci, &s, sizeof s, cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
     cases[ci].fresh = false;
+    cases[ci].dt_stale = true;
   }
   void* old[] = {d_blocks_, d_cases_, d_case_blk_, d_tasks_, d_partials_, d_pairs_, d_counters_, d_casemax_};
   for (void* p : old)
@@ -1160,8 +1164,26 @@ int Engine::prepare() {
   int rc = ensure_planned();
   if (rc) return rc;
   if (npairs > 0) CK(launch_gather(role_[ROLE_A], cap_, d_pairs_, npairs, stream));
-  CK(launch_init_dt(d_blocks_, (int)blocks.size(), d_cases_, d_state_, (int)cases.size(), d_casemax_, ROLE_A,
-                    stream));
+  // dt from the state only for cases whose state was uploaded since their
+  // last step (or that are new); a running case keeps the dt its last step
+  // computed, so adding or removing other cases does not change its results
+  std::vector<int> mask(cases.size(), 0);
+  bool any = false;
+  for (size_t c = 0; c < cases.size(); ++c)
+    if (!cases[c].dead && cases[c].dt_stale) mask[c] = 1, any = true;
+  if (any) {
+    if (dtmask_cap_ < (int)cases.size()) {
+      if (d_dtmask_) cudaFree(d_dtmask_);
+      d_dtmask_ = nullptr;
+      CK(cudaMalloc(&d_dtmask_, sizeof(int) * cases.size()));
+      dtmask_cap_ = (int)cases.size();
+    }
+    CK(cudaMemcpyAsync(d_dtmask_, mask.data(), sizeof(int) * cases.size(), cudaMemcpyHostToDevice, stream));
+    CK(launch_init_dt(d_blocks_, (int)blocks.size(), d_cases_, d_state_, (int)cases.size(), d_casemax_, d_dtmask_,
+                      ROLE_A, stream));
+    CK(cudaStreamSynchronize(stream));  // the mask's host copy goes out of scope
+    for (auto& c : cases) c.dt_stale = false;
+  }
   prepared_ = true;
   return FVM_OK;
 }
@@ -1179,6 +1201,7 @@ int Engine::set_state(int blk, const double* q) {
   CK(cudaMemcpyAsync(d_staging_, q, bytes, cudaMemcpyHostToDevice, stream));
   CK(launch_unpack(role_[ROLE_A] + b.slab_off + b.org, cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1], (int)b.n[2],
                    d_staging_, stream));
+  cases[b.case_id].dt_stale = true;
   // a new state clears the case's error status (NaN / divergence of an
   // earlier state)
   if (d_state_ && b.case_id < state_cap_ && !cases[b.case_id].fresh)

@@ -55,6 +55,7 @@ struct HCase {
   std::vector<int> blocks;
   bool dead = false;
   bool fresh = true;    // device state (time, residual history) not initialised
+  bool dt_stale = true; // state uploaded since the last step: dt is recomputed from it
   int group = -1;
   int tile = -1;        // forced tile (autotuner result), -1 = heuristic
   int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model
@@ -163,6 +164,8 @@ class Engine {
   int vlist_off_[6] = {0, 0, 0, 0, 0, 0}, vlist_n_[6] = {0, 0, 0, 0, 0, 0};
   std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..C][plane, z] (null: no TMA)
   int32_t* d_err_ = nullptr;          // kernel error flag (a tensor copy that did not arrive)
+  int* d_dtmask_ = nullptr;           // cases whose dt prepare() recomputes
+  int dtmask_cap_ = 0;
   bool drop_copies_ = false;          // test hook: tensor copies armed but not issued
   unsigned long long* d_casemax_ = nullptr;
   double* d_staging_ = nullptr;

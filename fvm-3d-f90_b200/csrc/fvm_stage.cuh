@@ -227,13 +227,23 @@ template <class R> __device__ __forceinline__ Prim5<R> mkprim(const R s[5]) {
 
 // Wave-speed sum of one cell, sum_d (|u_d| + c) / dr_d, from conservative
 // values, exact FP64 (the CFL time step of the host runtime).
+// EX: divisions and the IEEE square root; the other forms the reciprocal,
+// reciprocal square root and reciprocal cell sizes (idr).
+template <bool EX>
 __device__ __forceinline__ double wavespeed(const double q[5], double gamma, double gm1, const double dr[3],
-                                            int idim) {
-  Prim5<double> p = cons2prim<double, true>(q[0], q[1], q[2], q[3], q[4], gm1);
-  const double c = sqrt(gamma * p.p / p.r);
-  double s = (fabs(p.u) + c) / dr[0] + (fabs(p.v) + c) / dr[1];
-  if (idim == 3) s = s + (fabs(p.w) + c) / dr[2];
-  return s;
+                                            const double idr[3], int idim) {
+  Prim5<double> p = cons2prim<double, EX>(q[0], q[1], q[2], q[3], q[4], gm1);
+  if constexpr (EX) {
+    const double c = sqrt(gamma * p.p / p.r);
+    double s = (fabs(p.u) + c) / dr[0] + (fabs(p.v) + c) / dr[1];
+    if (idim == 3) s = s + (fabs(p.w) + c) / dr[2];
+    return s;
+  } else {
+    const double c = nsqrt_(gamma * p.p * rcp_(p.r));
+    double s = (fabs(p.u) + c) * idr[0] + (fabs(p.v) + c) * idr[1];
+    if (idim == 3) s = s + (fabs(p.w) + c) * idr[2];
+    return s;
+  }
 }
 
 // Deterministic CTA reduction of the column accumulators sS[6][NT] (5 sums,
@@ -368,6 +378,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
     const double dr0 = B.dr[0], dr1 = B.dr[1], dr2 = B.dr[2];
     const double idr0 = B.inv_dr[0], idr1 = B.inv_dr[1], idr2 = B.inv_dr[2];
     const double drv[3] = {dr0, dr1, dr2};
+    const double idrv[3] = {idr0, idr1, idr2};
     const int rk_stages = CS.rk_stages, ts_set = CS.timestep_set, idim = CS.idim;
     const double cfl = CS.cfl, gammad = CS.gamma;
     const double* visc = B.visc;
@@ -864,7 +875,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
           ac[v] = need_acc ? sQ[(1 * 5 + v) * NC + tid] : 0.0;
         }
         double h = dtg;
-        if (ts_set == 2) h = cfl / wavespeed(u0, gammad, gm1d, drv, idim);
+        if (ts_set == 2) h = cfl / wavespeed<EX>(u0, gammad, gm1d, drv, idrv, idim);
         double out[5];
         if (rk_stages == 3) {
           if (a.m == 1) {
@@ -905,7 +916,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         if (a.last) {
 #pragma unroll
           for (int v = 0; v < 5; ++v) sS[v * NT + tid] += rhs[v] * rhs[v];
-          if (ts_set != 0) sS[5 * NT + tid] = fmax(sS[5 * NT + tid], wavespeed(out, gammad, gm1d, drv, idim));
+          if (ts_set != 0) sS[5 * NT + tid] = fmax(sS[5 * NT + tid], wavespeed<EX>(out, gammad, gm1d, drv, idrv, idim));
           if (rhs_out) {
             const int64_t nc = (int64_t)G.n0 * G.n1 * G.n2;
             const int64_t r0 = gx + (int64_t)G.n0 * (gy + (int64_t)G.n1 * k);

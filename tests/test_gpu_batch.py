@@ -145,3 +145,26 @@ def test_navier_stokes_mixed_precisions_batched():
     o.step(3)
     assert np.array_equal(s.get_state(ids[0][0]), o.get_state(0))
     s.close()
+
+
+def test_running_case_unchanged_when_another_joins():
+    # a case that is stepping keeps the dt its last step computed when the
+    # engine re-plans for a joining case: 3 + 3 steps with a case added in
+    # between equal 6 steps alone (CFL time step, FP64 and FP32 forms)
+    for prec in (abi.PREC_FP64, abi.PREC_FP32_FLUX):
+        a = cases.isentropic_vortex(N=16, layout="blocks8", rk_stages=3, precision=prec,
+                                    timestep_set=abi.DT_CFL, cfl=0.5)
+        b = cases.blast((16, 16, 16), seed=4, precision=prec)
+        ref = alone(a, 6)
+        s = Solver(a.config())
+        s.remove_case(0)
+        ca = s.add_case(a.config())
+        a.apply(s, case_id=ca)
+        ids = list(a.block_ids)
+        s.step(3)
+        cb = s.add_case(b.config())
+        b.apply(s, case_id=cb)
+        s.step(3)
+        for k, g in enumerate(ids):
+            assert np.array_equal(s.get_state(g), ref[k]), (prec, k)
+        s.close()
