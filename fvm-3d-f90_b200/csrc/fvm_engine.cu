@@ -993,7 +993,7 @@ int Engine::plan() {
     if (!G.k.tma) continue;
     PFN_cuTensorMapEncodeTiled enc = encode_fn();
     if (!enc) return fail(FVM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    std::vector<CUtensorMap> maps(blocks.size() * 3 * 2);
+    std::vector<CUtensorMap> maps(blocks.size() * NROLE * 2);
     std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
     for (int ci : live_cases) {
       if (cases[ci].group != (int)g) continue;
@@ -1004,10 +1004,10 @@ int Engine::plan() {
         const cuuint32_t box_p[4] = {(cuuint32_t)G.k.box_w, (cuuint32_t)G.k.box_h, 1, 5};
         const cuuint32_t box_z[4] = {(cuuint32_t)G.k.tx, (cuuint32_t)G.k.ty, 1, 5};
         const cuuint32_t estr[4] = {1, 1, 1, 1};
-        for (int r = 0; r < 3; ++r) {
+        for (int r = 0; r < NROLE; ++r) {
           void* base = role_[r] + b.slab_off;
           for (int w = 0; w < 2; ++w) {
-            const CUresult e = enc(&maps[((size_t)bi * 3 + r) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+            const CUresult e = enc(&maps[((size_t)bi * NROLE + r) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
                                    strides, w == 0 ? box_p : box_z, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);

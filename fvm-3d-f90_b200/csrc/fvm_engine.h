@@ -162,7 +162,7 @@ class Engine {
   int ncounters_ = 0;
   // viscous task lists in d_tasks_, index precision * 2 + (3D ? 0 : 1)
   int vlist_off_[6] = {0, 0, 0, 0, 0, 0}, vlist_n_[6] = {0, 0, 0, 0, 0, 0};
-  std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..C][plane, z] (null: no TMA)
+  std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..ACC][plane, z] (null: no TMA)
   int32_t* d_err_ = nullptr;          // kernel error flag (a tensor copy that did not arrive)
   int* d_dtmask_ = nullptr;           // cases whose dt prepare() recomputes
   int dtmask_cap_ = 0;

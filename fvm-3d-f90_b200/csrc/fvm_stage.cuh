@@ -77,6 +77,9 @@ struct StageCfg {
   // x / y halo, [5][PH][TW] with TW = TX + 2H + 1 rounded up to even (the
   // box starts on an even x, so its first coordinate is 16-byte aligned),
   // and the z window's next plane, [5][TY][TX]; both padded to 128 bytes.
+  // These kernels also take the RK operands of plane k as [5][TY][TX] boxes
+  // (the layout of the operand arrays), which keeps the per-thread copies
+  // and their L1 lines out of the plane loop.
   static constexpr bool TMA = PSM && DIM == 3;
   static constexpr int TW = (TX + 2 * H + 2) / 2 * 2;
   static constexpr int TPB = (5 * PH * TW + 15) / 16 * 16;
@@ -327,8 +330,8 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
   double* sTZ = sTP + C::TPB;                                         // TMA: [5][TY][TX] z window's next plane
   __shared__ double s_red[6 * (NT / 32)];
   __shared__ int s_task;
-  __shared__ __align__(8) uint64_t s_mbar[2];  // TMA: plane box, z box
-  uint32_t ph_p = 0, ph_z = 0;                 // TMA: expected phase parity of each mbarrier
+  __shared__ __align__(8) uint64_t s_mbar[3];  // TMA: plane box, z box, RK operands
+  uint32_t ph_p = 0, ph_z = 0, ph_q = 0;       // TMA: expected phase parity of each mbarrier
 
   const int tid = threadIdx.x;
   // column threads own a z column; the others (whole warps) skip all z work
@@ -338,6 +341,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
     if (tid == 0) {
       mbar_init(&s_mbar[0], 1);
       mbar_init(&s_mbar[1], 1);
+      mbar_init(&s_mbar[2], 1);
       mbar_fence_init();
     }
     __syncthreads();
@@ -425,8 +429,13 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       xy_clamp(G, x, y);
       zsrc = (y - T.y0) * TX + (x - T.x0);
     }
+    // tensor maps of this block: [role][plane box, z-shaped box]
+    const CUtensorMap* tmb = nullptr;
     const CUtensorMap* tmp = nullptr;
-    if constexpr (C::TMA) tmp = a.tmap + ((int64_t)T.blk * 3 + a.rin) * 2;
+    if constexpr (C::TMA) {
+      tmb = a.tmap + (int64_t)T.blk * NROLE * 2;
+      tmp = tmb + a.rin * 2;
+    }
 
     // ---- z window (3D) --------------------------------------------------
     R zw[C::WIN][5];
@@ -509,9 +518,21 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       if constexpr (C::PSM && !C::TMA) __pipeline_commit();
 
       // ---- the cell's RK operands of plane k, copied asynchronously into
-      // shared memory; phase C waits for this thread's own copies only.
+      // shared memory (TMA boxes, or per-thread copies of which phase C
+      // waits for this thread's own only)
       const int64_t off_k = (int64_t)gx + (int64_t)gy * G.sy + (int64_t)k * G.sz;
-      if (do_xy && act) {
+      if constexpr (C::TMA) {
+        // TMA kernels: the operands of the whole tile as [5][TY][TX] boxes of
+        // plane k (the layout of sQ), straight into shared memory
+        if (do_xy && tid == 0) {
+          const int nb = 1 + ((need_um || need_acc) ? 1 : 0);
+          mbar_expect_tx(&s_mbar[2], sizeof(double) * 5 * TY * TX * nb);
+          const int bx = T.x0 + kPadX, by = T.y0 + kGhost, bz = k + kGhost;
+          tma_load_4d(sQ, tmb + a.rq0 * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
+          if (need_um) tma_load_4d(sQ + 5 * NC, tmb + a.rin * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
+          if (need_acc) tma_load_4d(sQ + 5 * NC, tmb + a.racc * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
+        }
+      } else if (do_xy && act) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
           __pipeline_memcpy_async(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs, sizeof(double));
@@ -831,6 +852,18 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       __syncthreads();
 
       // ---- phase C: rhs, RK update, reductions -------------------------------
+      if constexpr (C::TMA) {
+        // every thread waits for the operand boxes issued at the top of this
+        // plane (they leave together if a box does not arrive)
+        if (do_xy) {
+          const bool okq = mbar_wait(&s_mbar[2], ph_q);
+          ph_q ^= 1;
+          if (!okq) {
+            if (tid == 0) atomicExch(a.err, 1);
+            return;
+          }
+        }
+      }
       if (do_xy && act) {
         constexpr int NF = C::NXF + C::NYF;
         const int fxl = ty * (TX + 1) + tx;
@@ -867,7 +900,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         }
         // RK update (scheme_Runge_Kutta.f90:30-63; classic RK4 for 4 stages)
         double u0[5], um[5], ac[5];
-        __pipeline_wait_prior(0);
+        if constexpr (!C::TMA) __pipeline_wait_prior(0);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
           u0[v] = sQ[(0 * 5 + v) * NC + tid];

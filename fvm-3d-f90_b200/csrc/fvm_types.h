@@ -88,7 +88,7 @@ struct StageArgs {
   int32_t m;                   // RK stage, 1-based
   int32_t rin, rout, rq0, racc;
   int32_t last;                // last stage of the step: residual + wave speed
-  // tensor maps of the prefetching 3D kernels, [block][role A..C][plane, z]
+  // tensor maps of the prefetching 3D kernels, [block][role A..ACC][plane, z]
   // (null for kernels that load with per-thread copies)
   const CUtensorMap* tmap;
   int32_t* err;                // set to 1 when a tensor copy does not arrive
