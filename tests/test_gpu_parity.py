@@ -79,7 +79,7 @@ def test_3d_multiblock_exact_bitwise(recon, flux, stages, compat):
     np.testing.assert_allclose(rag, rao, rtol=1e-12)
 
 
-@pytest.mark.parametrize("tile,zchunk", [(0, 5), (1, 8), (0, 0)])
+@pytest.mark.parametrize("tile,zchunk", [(0, 5), (1, 8), (0, 0), (3, 7), (3, 0)])
 def test_tiling_does_not_change_state(tile, zchunk):
     c = cases.isentropic_vortex(N=32, layout="blocks8")
     o = c.apply(orc.Oracle(c.config()))
@@ -95,6 +95,26 @@ def test_tiling_does_not_change_state(tile, zchunk):
     g.step(2)
     for b in range(8):
         assert np.array_equal(g.get_state(b), o.get_state(b))
+
+
+@pytest.mark.parametrize("recon,flux", [(abi.RECON_MUSCL, abi.FLUX_ROE), (abi.RECON_WENO, abi.FLUX_VANLEER)])
+def test_tma_tile_rk3_exact(recon, flux):
+    # the 16x8 tile (plane, z window and RK operands by tensor copies) in the
+    # exact form, SSP-RK3 (q_in operand), 8 uneven periodic blocks
+    from fvm3d import tuning
+
+    c = cases.isentropic_vortex(N=24, layout="blocks8", rk_stages=3, reconstruct=recon, flux_split=flux,
+                                limiter=abi.LIMITER_VANALBADA, kappa=1.0 / 3.0)
+    o = c.apply(orc.Oracle(c.config()))
+    o.step(3)
+    g = Solver(c.config())
+    c.apply(g, states=False)
+    tuning.set_tuning(g, 0, 3, 5)
+    for b, q in enumerate(c.states):
+        g.set_state(b, q)
+    g.step(3)
+    for b in range(8):
+        assert np.array_equal(g.get_state(b), o.get_state(b)), f"block {b}"
 
 
 def test_local_timestep_exact():
