@@ -56,8 +56,9 @@ def parse():
     ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk with --tile")
     ap.add_argument("--forms", default="fp32,fp64,exact",
                     help="comma list of arms: fp32 (headline), fp64, exact")
-    ap.add_argument("--only", choices=["tgv", "riemann2d"], default=None,
+    ap.add_argument("--only", choices=["tgv", "riemann2d", "accuracy"], default=None,
                     help="run one secondary leg alone (its precision forms from --forms) and print its JSON")
+    ap.add_argument("--accuracy-steps", type=int, default=1000, help="RK4 steps of the accuracy leg")
     return ap.parse_args()
 
 
@@ -400,6 +401,42 @@ def tgv(args):
     return out
 
 
+# ---------------------------------------------------------------- accuracy leg
+def accuracy_leg(args):
+    """The vortex workload run for --accuracy-steps RK4 steps (CFL 0.5) in the
+    exact, FP64 and FP32-flux forms and both compat modes: L1 (mean) and Linf
+    density error against the exact solution (the vortex translated by the
+    free stream to each run's own final time) and against the exact form,
+    which is bit-identical to the oracle."""
+    import numpy as np
+
+    from fvm3d import abi, cases
+    from fvm3d.solver import Solver
+
+    c = cases.isentropic_vortex(N=args.n, layout="blocks8")
+    steps = args.accuracy_steps
+    out = {"cells": c.ncells, "steps": steps}
+    for cname, compat in (("reference", abi.COMPAT_REFERENCE), ("textbook", abi.COMPAT_TEXTBOOK)):
+        runs = {}
+        for name, prec in (("exact", abi.PREC_FP64_EXACT), ("fp64", abi.PREC_FP64), ("fp32_flux", abi.PREC_FP32_FLUX)):
+            s = c.apply(Solver(c.config(precision=prec, compat=compat)))
+            t0 = time.perf_counter()
+            t, _, _ = s.step(steps)
+            sec = time.perf_counter() - t0
+            rho = np.concatenate([s.get_state(b)[0].ravel() for b in range(len(c.blocks))])
+            s.close()
+            ex = np.concatenate([q[0].ravel() for q in cases.vortex_exact(c, t)])
+            runs[name] = rho
+            e = np.abs(rho - ex)
+            out.setdefault(cname, {})[name] = {"t_end": t, "l1_vs_exact_solution": float(e.mean()),
+                                               "linf_vs_exact_solution": float(e.max()), "wall_s": round(sec, 3)}
+        for name in ("fp64", "fp32_flux"):
+            d = np.abs(runs[name] - runs["exact"])
+            out[cname][name]["l1_vs_exact_form"] = float(d.mean())
+            out[cname][name]["linf_vs_exact_form"] = float(d.max())
+    return out
+
+
 # ---------------------------------------------------------------- 2D Riemann leg
 def riemann2d_leg(args):
     """Four-quadrant 2D Riemann problem on 256 x 256 nodes of [0,1]^2, one
@@ -503,7 +540,7 @@ def main():
         return
 
     if args.only:
-        leg = {"tgv": tgv, "riemann2d": riemann2d_leg}[args.only]
+        leg = {"tgv": tgv, "riemann2d": riemann2d_leg, "accuracy": accuracy_leg}[args.only]
         if dist.rank == 0:
             print(json.dumps({"leg": args.only, **leg(args)}))
         dist.close()

@@ -117,6 +117,17 @@ def test_tma_tile_rk3_exact(recon, flux):
         assert np.array_equal(g.get_state(b), o.get_state(b)), f"block {b}"
 
 
+@pytest.mark.parametrize("compat", [abi.COMPAT_REFERENCE, abi.COMPAT_TEXTBOOK])
+def test_long_run_exact_bitwise(compat):
+    # 300 CFL steps of the 8-block vortex: the exact form stays bit-identical
+    # to the oracle (dt history, ghost exchange and residual state included)
+    c = cases.isentropic_vortex(N=16, layout="blocks8", compat=compat)
+    g, o, (tg, _, _), (to, _, _, _) = run_both(c, 300)
+    assert tg == to
+    for b in range(8):
+        assert np.array_equal(g.get_state(b), o.get_state(b)), f"block {b}"
+
+
 def test_local_timestep_exact():
     c = cases.isentropic_vortex(N=16, layout="blocks8", timestep_set=abi.DT_CFL_LOCAL, rk_stages=3,
                                 reconstruct=abi.RECON_MUSCL, limiter=abi.LIMITER_VANLEER, flux_split=abi.FLUX_ROE)
