@@ -87,6 +87,9 @@ Engine::~Engine() {
   release();
   for (auto s : side_) cudaStreamDestroy(s);
   for (auto e : fork_ev_) cudaEventDestroy(e);
+  for (auto e : xev_)
+    if (e) cudaEventDestroy(e);
+  if (xstream_) cudaStreamDestroy(xstream_);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -119,6 +122,9 @@ void Engine::release() {
   d_casemax_ = nullptr;
   d_staging_ = nullptr;
   staging_bytes_ = 0;
+  if (d_staging2_) cudaFree(d_staging2_);
+  d_staging2_ = nullptr;
+  staging2_bytes_ = 0;
   for (auto p : d_tmap_)
     if (p) cudaFree(p);
   d_tmap_.clear();
@@ -1229,6 +1235,103 @@ int Engine::get_state(int blk, double* q, int prim) {
   return FVM_OK;
 }
 
+// The second staging buffer, the copy stream and its events, made on first
+// use of set_states / get_states.
+int Engine::ensure_xfer() {
+  if (staging2_bytes_ < staging_bytes_) {
+    if (d_staging2_) cudaFree(d_staging2_);
+    d_staging2_ = nullptr;
+    staging2_bytes_ = 0;
+    CK(cudaMalloc(&d_staging2_, staging_bytes_));
+    staging2_bytes_ = staging_bytes_;
+  }
+  if (!xstream_) CK(cudaStreamCreateWithFlags(&xstream_, cudaStreamNonBlocking));
+  for (auto& e : xev_)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return FVM_OK;
+}
+
+// fvm_set_state for n blocks: block i goes through staging buffer i % 2; its
+// host-to-device copy (on xstream_) waits only for the unpack of block i - 2,
+// so the copies run back to back while the engine stream unpacks. One
+// synchronisation at the end: the host buffers are not read after return.
+int Engine::set_states(int n, const int* blk, const double* const* q) {
+  if (n < 0 || (n > 0 && (!blk || !q))) return fail(FVM_ERR_INVALID, "bad block list");
+  for (int i = 0; i < n; ++i) {
+    if (!live_block(blk[i])) return fail(FVM_ERR_INVALID, "bad block id");
+    if (!q[i]) return fail(FVM_ERR_INVALID, "null state");
+  }
+  if (n == 0) return FVM_OK;
+  if (!laid_out_) {
+    int rc = layout();
+    if (rc) return rc;
+  }
+  int rc = ensure_xfer();
+  if (rc) return rc;
+  double* stg[2] = {d_staging_, d_staging2_};
+  cudaEvent_t* copied = xev_;
+  cudaEvent_t* used = xev_ + 2;
+  CK(cudaEventRecord(xev_[4], stream));  // earlier work on the engine stream may read the staging buffers
+  CK(cudaStreamWaitEvent(xstream_, xev_[4], 0));
+  for (int i = 0; i < n; ++i) {
+    const int j = i & 1;
+    const HBlock& b = blocks[blk[i]];
+    const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
+    if (i >= 2) CK(cudaStreamWaitEvent(xstream_, used[j], 0));
+    CK(cudaMemcpyAsync(stg[j], q[i], bytes, cudaMemcpyHostToDevice, xstream_));
+    CK(cudaEventRecord(copied[j], xstream_));
+    CK(cudaStreamWaitEvent(stream, copied[j], 0));
+    CK(launch_unpack(role_[ROLE_A] + b.slab_off + b.org, cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1],
+                     (int)b.n[2], stg[j], stream));
+    CK(cudaEventRecord(used[j], stream));
+    cases[b.case_id].dt_stale = true;
+    if (d_state_ && b.case_id < state_cap_ && !cases[b.case_id].fresh)
+      CK(cudaMemsetAsync(reinterpret_cast<char*>(d_state_ + b.case_id) + offsetof(DevCaseState, status), 0,
+                         sizeof(int32_t), stream));
+  }
+  CK(cudaStreamSynchronize(stream));
+  prepared_ = false;
+  return FVM_OK;
+}
+
+// fvm_get_state for n blocks: the engine stream packs block i into staging
+// buffer i % 2 once the device-to-host copy of block i - 2 (on xstream_) has
+// left it; one synchronisation at the end.
+int Engine::get_states(int n, const int* blk, double* const* q) {
+  if (n < 0 || (n > 0 && (!blk || !q))) return fail(FVM_ERR_INVALID, "bad block list");
+  for (int i = 0; i < n; ++i) {
+    if (!live_block(blk[i])) return fail(FVM_ERR_INVALID, "bad block id");
+    if (!q[i]) return fail(FVM_ERR_INVALID, "null output");
+  }
+  if (n == 0) return FVM_OK;
+  if (!laid_out_) {
+    if (cap_ == 0) return fail(FVM_ERR_STATE, "no state uploaded yet");
+    int rc = layout();
+    if (rc) return rc;
+  }
+  int rc = ensure_xfer();
+  if (rc) return rc;
+  double* stg[2] = {d_staging_, d_staging2_};
+  cudaEvent_t* copied = xev_;
+  cudaEvent_t* used = xev_ + 2;
+  for (int i = 0; i < n; ++i) {
+    const int j = i & 1;
+    const HBlock& b = blocks[blk[i]];
+    const size_t bytes = sizeof(double) * 5 * b.n[0] * b.n[1] * b.n[2];
+    if (i >= 2) CK(cudaStreamWaitEvent(stream, copied[j], 0));
+    CK(launch_pack(role_[ROLE_A] + b.slab_off + b.org, cap_, (int)b.sy, (int)b.sz, (int)b.n[0], (int)b.n[1],
+                   (int)b.n[2], stg[j], 0, cases[b.case_id].cfg.gamma - 1.0, stream));
+    CK(cudaEventRecord(used[j], stream));
+    CK(cudaStreamWaitEvent(xstream_, used[j], 0));
+    CK(cudaMemcpyAsync(q[i], stg[j], bytes, cudaMemcpyDeviceToHost, xstream_));
+    CK(cudaEventRecord(copied[j], xstream_));
+  }
+  CK(cudaEventRecord(xev_[4], xstream_));
+  CK(cudaStreamWaitEvent(stream, xev_[4], 0));  // later engine work may reuse the staging buffers
+  CK(cudaStreamSynchronize(xstream_));
+  return FVM_OK;
+}
+
 int Engine::get_rhs(int blk, double* rhs) {
   if (!live_block(blk)) return fail(FVM_ERR_INVALID, "bad block id");
   if (!rhs) return fail(FVM_ERR_INVALID, "null output");
@@ -1380,6 +1483,16 @@ int fvm_set_state(fvm_ctx* ctx, int blk, const double* q) {
 int fvm_get_state(fvm_ctx* ctx, int blk, double* q) {
   if (!ctx) return FVM_ERR_INVALID;
   return ctx->eng.get_state(blk, q, 0);
+}
+
+int fvm_set_states(fvm_ctx* ctx, int n, const int* blk, const double* const* q) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.set_states(n, blk, q);
+}
+
+int fvm_get_states(fvm_ctx* ctx, int n, const int* blk, double* const* q) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.get_states(n, blk, q);
 }
 
 int fvm_get_primitive(fvm_ctx* ctx, int blk, double* p) {

@@ -89,6 +89,9 @@ class Engine {
 
   int set_state(int blk, const double* q);
   int get_state(int blk, double* q, int prim);
+  // several blocks per call: copies on xstream_ overlap the (un)packing
+  int set_states(int n, const int* blk, const double* const* q);
+  int get_states(int n, const int* blk, double* const* q);
   int get_rhs(int blk, double* rhs);
   int step(int nsteps);
   int read_case_state(int case_id, DevCaseState* out);
@@ -170,6 +173,11 @@ class Engine {
   unsigned long long* d_casemax_ = nullptr;
   double* d_staging_ = nullptr;
   size_t staging_bytes_ = 0;
+  double* d_staging2_ = nullptr;      // second staging buffer of set_states / get_states
+  size_t staging2_bytes_ = 0;
+  cudaStream_t xstream_ = nullptr;    // their host <-> device copies
+  cudaEvent_t xev_[5] = {};           // copied[2], used[2], start
+  int ensure_xfer();
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
   std::vector<cudaStream_t> side_;  // fork streams for parallel group launches

@@ -165,6 +165,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "fvm_connect": (ctypes.c_int, [vp, ctypes.c_int, P(i64), ctypes.c_int, P(i64), P(i32)]),
         "fvm_set_state": (ctypes.c_int, [vp, ctypes.c_int, P(dbl)]),
         "fvm_get_state": (ctypes.c_int, [vp, ctypes.c_int, P(dbl)]),
+        "fvm_set_states": (ctypes.c_int, [vp, ctypes.c_int, P(ctypes.c_int), P(P(dbl))]),
+        "fvm_get_states": (ctypes.c_int, [vp, ctypes.c_int, P(ctypes.c_int), P(P(dbl))]),
         "fvm_get_primitive": (ctypes.c_int, [vp, ctypes.c_int, P(dbl)]),
         "fvm_get_rhs": (ctypes.c_int, [vp, ctypes.c_int, P(dbl)]),
         "fvm_step": (ctypes.c_int, [vp, ctypes.c_int, P(dbl), P(dbl), P(dbl)]),

@@ -142,6 +142,38 @@ class Solver:
     def get_state_ptr(self, blk: int, ptr: int):
         self._chk(self.lib.fvm_get_state(self.h, blk, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double))))
 
+    def _many(self, fn, blks, ptrs):
+        n = len(blks)
+        ids = (ctypes.c_int * n)(*blks)
+        arr = (ctypes.POINTER(ctypes.c_double) * n)(*[ctypes.cast(p, ctypes.POINTER(ctypes.c_double)) for p in ptrs])
+        self._chk(fn(self.h, n, ids, arr))
+
+    def set_states_ptr(self, blks, ptrs):
+        """Upload several blocks in one call (fvm_set_states) from raw host
+        pointers, e.g. pinned memory; copies overlap the unpacking."""
+        self._many(self.lib.fvm_set_states, list(blks), list(ptrs))
+
+    def get_states_ptr(self, blks, ptrs):
+        """Download several blocks in one call (fvm_get_states)."""
+        self._many(self.lib.fvm_get_states, list(blks), list(ptrs))
+
+    def set_states(self, qs: dict):
+        """Upload {block: q} with q as set_state takes it, in one call."""
+        arrs = {}
+        for blk, q in qs.items():
+            ni, nj, nk = self._shape(blk)
+            arrs[blk] = np.ascontiguousarray(q, dtype=np.float64).reshape(5, nk, nj, ni)
+        self.set_states_ptr(list(arrs), [a.ctypes.data for a in arrs.values()])
+
+    def get_states(self, blks) -> list:
+        """The conservative states of blocks `blks`, in one call."""
+        outs = []
+        for blk in blks:
+            ni, nj, nk = self._shape(blk)
+            outs.append(np.empty((5, nk, nj, ni), dtype=np.float64))
+        self.get_states_ptr(list(blks), [o.ctypes.data for o in outs])
+        return outs
+
     def _get(self, fn, blk):
         ni, nj, nk = self._shape(blk)
         out = np.empty((5, nk, nj, ni), dtype=np.float64)

@@ -160,6 +160,15 @@ int fvm_connect(fvm_ctx* ctx, int blk, const int64_t range[3][2], int donor,
 int fvm_set_state(fvm_ctx* ctx, int blk, const double* q);
 /* Download the conservative state of one block (layout above). */
 int fvm_get_state(fvm_ctx* ctx, int blk, double* q);
+/* The same for n blocks at once (q[i] is block blk[i]'s array, as above):
+ * the per-block get_q() / set_q() exchanges of the reference
+ * (src/base/defs_block_data.f90:299-312) in one call. The host-device copies
+ * of consecutive blocks run back to back on a copy stream while the library
+ * (un)packs the neighbouring block, and the call synchronises once, so the
+ * host arrays are not touched after it returns. Results equal n calls of
+ * fvm_set_state / fvm_get_state. */
+int fvm_set_states(fvm_ctx* ctx, int n, const int* blk, const double* const* q);
+int fvm_get_states(fvm_ctx* ctx, int n, const int* blk, double* const* q);
 /* Download primitives (rho,u,v,w,p) of one block, same layout, computed as
  * convert_q_to_p_blk_sub (class_flow_field.f90:383-396). */
 int fvm_get_primitive(fvm_ctx* ctx, int blk, double* p);

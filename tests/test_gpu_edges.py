@@ -114,3 +114,31 @@ def test_fast_fp64_reciprocals_within_2ulp():
     ulp_rs = np.abs(rs - ref_rs) / np.spacing(ref_rs)
     assert ulp_r.max() <= 2.0, ulp_r.max()
     assert ulp_rs.max() <= 2.0, ulp_rs.max()
+
+
+def test_multi_block_state_calls_match_per_block():
+    # fvm_set_states / fvm_get_states (copies of consecutive blocks overlap the
+    # unpacking) give exactly what per-block fvm_set_state / fvm_get_state
+    # give, with the blocks in any order, repeated calls, and bad arguments
+    # rejected before any copy
+    c = cases.isentropic_vortex(N=24, layout="blocks8", precision=abi.PREC_FP32_FLUX)
+    a = c.apply(Solver(c.config()))
+    b = Solver(c.config())
+    c.apply(b, states=False)
+    order = [5, 0, 7, 2, 1, 6, 3, 4]
+    b.set_states({k: c.states[k] for k in order})
+    for s in (a, b):
+        s.step(2)
+    got = b.get_states(order)
+    for k, g in zip(order, got):
+        assert np.array_equal(g, a.get_state(k))
+    b.set_states({k: got[i] for i, k in enumerate(order)})
+    again = b.get_states(list(range(8)))
+    for k in range(8):
+        assert np.array_equal(again[k], a.get_state(k))
+    with pytest.raises(FvmError) as e:
+        b.get_states_ptr([0, 99], [again[0].ctypes.data, again[1].ctypes.data])
+    assert e.value.code == 1
+    b.set_states({})
+    a.close()
+    b.close()
