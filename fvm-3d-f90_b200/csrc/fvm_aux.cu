@@ -18,13 +18,32 @@ namespace fvm {
 // Ghost cells of connected / periodic regions: dst[i] = src[i] for all five
 // variables, offsets relative to a role slab (the block-to-block exchange the
 // reference describes in defs_face_geom.f90:378-402 but never performs).
-__global__ void gather_kernel(double* __restrict__ base, int64_t vs, const int64_t* __restrict__ pairs,
+// Every source is a real cell (the host resolves ghost-to-ghost chains), so
+// the pairs are independent. Each thread takes kGatherPer pairs a grid
+// apart (a warp's pairs stay consecutive) and issues all their loads before
+// any store, so the index-then-data latency chain is paid once per thread.
+constexpr int kGatherPer = 4;
+__global__ void gather_kernel(double* __restrict__ base, int64_t vs, const longlong2* __restrict__ pairs,
                               int64_t npairs) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npairs;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t d = pairs[2 * i], s = pairs[2 * i + 1];
+  const int64_t G = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += G * kGatherPer) {
+    longlong2 p[kGatherPer];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) base[d + v * vs] = base[s + v * vs];
+    for (int j = 0; j < kGatherPer; ++j) {
+      const int64_t i = i0 + j * G;
+      p[j] = i < npairs ? pairs[i] : make_longlong2(-1, -1);
+    }
+    double val[kGatherPer][5];
+#pragma unroll
+    for (int j = 0; j < kGatherPer; ++j)
+      if (p[j].x >= 0)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) val[j][v] = base[p[j].y + v * vs];
+#pragma unroll
+    for (int j = 0; j < kGatherPer; ++j)
+      if (p[j].x >= 0)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) base[p[j].x + v * vs] = val[j][v];
   }
 }
 
@@ -194,7 +213,8 @@ static inline int grid_for(int64_t n, int bs) {
 
 cudaError_t launch_gather(double* base, int64_t vs, const int64_t* pairs, int64_t npairs, cudaStream_t s) {
   if (npairs == 0) return cudaSuccess;
-  gather_kernel<<<grid_for(npairs, 256), 256, 0, s>>>(base, vs, pairs, npairs);
+  const int64_t threads = (npairs + kGatherPer - 1) / kGatherPer;
+  gather_kernel<<<grid_for(threads, 256), 256, 0, s>>>(base, vs, reinterpret_cast<const longlong2*>(pairs), npairs);
   return cudaGetLastError();
 }
 
