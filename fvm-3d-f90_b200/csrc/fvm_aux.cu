@@ -149,12 +149,30 @@ __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, co
     const int bb = b0 + warp;
     if (warp < NW && bb < C.nblocks) {
       const DevBlock& B = blocks[case_blk[C.block0 + bb]];
+      // each lane loads kU partials before adding them (in a fixed order), so
+      // a block of many tasks costs one memory round trip per 32 * kU tasks
+      constexpr int kU = 8;
       double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
-      for (int t = lane; t < B.ntask; t += 32) {
-        const double* p = partials + (int64_t)(B.task0 + t) * kPartStride;
+      for (int t = lane; t < B.ntask; t += 32 * kU) {
+        double q[kU][6];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) s[v] += p[v];
-        m = fmax(m, p[5]);
+        for (int u = 0; u < kU; ++u) {
+          const int tt = t + 32 * u;
+          if (tt < B.ntask) {
+            const double* p = partials + (int64_t)(B.task0 + tt) * kPartStride;
+#pragma unroll
+            for (int v = 0; v < 6; ++v) q[u][v] = p[v];
+          } else {
+#pragma unroll
+            for (int v = 0; v < 6; ++v) q[u][v] = 0.0;  // adds nothing: same sums as task by task
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+#pragma unroll
+          for (int v = 0; v < 5; ++v) s[v] += q[u][v];
+          m = fmax(m, q[u][5]);
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
