@@ -18,11 +18,14 @@ cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* c
 cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                             int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s);
 // Viscous contribution of the Navier-Stokes blocks: one CTA per task of a
-// viscous task list (kViscTX x kViscTY column tiles over z ranges), all of
-// dimension idim and precision form prec (PREC_*). visc_occupancy: CTAs of
-// the 3D kernel of that form resident on one SM. The *_fast entry points
-// serve the FP64 and FP32 forms.
-constexpr int kViscTX = 16, kViscTY = 8;
+// viscous task list (column tiles over z ranges), all of dimension idim and
+// precision form prec (PREC_*). The tile is 16 x 8 for the FP64 forms and
+// 32 x 4 for the FP32 form, whose warps then read one row of 32 floats
+// (bank-conflict free; two 16-float rows 18 floats apart share two banks).
+// visc_occupancy: CTAs of the 3D kernel of that form resident on one SM. The
+// *_fast entry points serve the FP64 and FP32 forms.
+constexpr int visc_tx(int prec) { return prec == 2 ? 32 : 16; }
+constexpr int visc_ty(int prec) { return prec == 2 ? 4 : 8; }
 cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
                         int prec, int role, cudaStream_t s);
 cudaError_t visc_occupancy(int prec, int* ctas_per_sm);

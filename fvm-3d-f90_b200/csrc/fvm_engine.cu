@@ -789,6 +789,7 @@ int Engine::plan() {
   for (int prec = 0; prec < 3; ++prec) {
     for (int dim : {3, 2}) {
       const int li = prec * 2 + (dim == 3 ? 0 : 1);
+      const int64_t vtx = visc_tx(prec), vty = visc_ty(prec);
       vlist_off_[li] = (int)tasks.size();
       std::vector<const HBlock*> ns;
       for (int bi : live_blocks) {
@@ -807,7 +808,7 @@ int Engine::plan() {
           cost.clear();
           double longest = 0.0;
           for (const HBlock* b : ns) {
-            const int64_t ncol = ((b->n[0] + kViscTX - 1) / kViscTX) * ((b->n[1] + kViscTY - 1) / kViscTY);
+            const int64_t ncol = ((b->n[0] + vtx - 1) / vtx) * ((b->n[1] + vty - 1) / vty);
             equal_chunks(b->n[2], cand, z0s);
             for (size_t c = 0; c + 1 < z0s.size(); ++c)
               for (int64_t q = 0; q < ncol; ++q) {
@@ -829,8 +830,8 @@ int Engine::plan() {
         else
           z0s = {0, b->n[2]};
         for (size_t ch = 0; ch + 1 < z0s.size(); ++ch)
-          for (int64_t y0 = 0; y0 < b->n[1]; y0 += kViscTY)
-            for (int64_t x0 = 0; x0 < b->n[0]; x0 += kViscTX) {
+          for (int64_t y0 = 0; y0 < b->n[1]; y0 += vty)
+            for (int64_t x0 = 0; x0 < b->n[0]; x0 += vtx) {
               Task t;
               t.blk = bi;
               t.x0 = (int)x0;

@@ -108,7 +108,7 @@ __device__ __forceinline__ void visc_flux(const VPrimT<T>& L, const VPrimT<T>& R
 // cell (x face, y face) and the z face above it; its own column's primitives
 // stay in registers, and the neighbour values the three faces share are read
 // once. The faces on the high edges of the tile (x = TX, y = TY) are
-// computed by the first warp. x / y face fluxes meet in shared memory, the
+// computed by the first TX + TY threads. x / y face fluxes meet in shared memory, the
 // z face below is carried in registers. The conserved values of the next
 // two planes are copied asynchronously into two staging buffers while the
 // current plane's faces are computed; each thread converts the cells it
@@ -122,7 +122,7 @@ struct ViscCfg {
   static constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1), NF = NXF + NYF;
   static constexpr int NR = IDIM == 3 ? 3 : 1;      // primitive planes in the ring
   static constexpr int NPT = (PL + NT - 1) / NT;    // staged cells per thread
-  static_assert(TX + TY <= 32, "the high-edge faces are one warp's work");
+  static_assert(TX + TY <= NT, "one high-edge face per thread");
   // bytes for arithmetic type R of RB bytes: primitive ring, face fluxes,
   // two staging planes of FP64 conserved values
   template <int RB>
@@ -378,19 +378,20 @@ __global__ void __launch_bounds__(TX* TY, ViscMinBlocks<PREC>::v)
 template <int PREC>
 cudaError_t launch_visc_prec(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
                              int role, cudaStream_t s) {
+  constexpr int TX = visc_tx(PREC), TY = visc_ty(PREC);
   if (ntasks == 0) return cudaSuccess;
   if (idim == 3)
-    visc_tile_kernel<kViscTX, kViscTY, 3, PREC><<<ntasks, kViscTX * kViscTY, 0, s>>>(blocks, cases, tasks, role);
+    visc_tile_kernel<TX, TY, 3, PREC><<<ntasks, TX * TY, 0, s>>>(blocks, cases, tasks, role);
   else
-    visc_tile_kernel<kViscTX, kViscTY, 2, PREC><<<ntasks, kViscTX * kViscTY, 0, s>>>(blocks, cases, tasks, role);
+    visc_tile_kernel<TX, TY, 2, PREC><<<ntasks, TX * TY, 0, s>>>(blocks, cases, tasks, role);
   return cudaGetLastError();
 }
 
 template <int PREC>
 cudaError_t visc_occupancy_prec(int* ctas_per_sm) {
+  constexpr int TX = visc_tx(PREC), TY = visc_ty(PREC);
   int occ = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, visc_tile_kernel<kViscTX, kViscTY, 3, PREC>,
-                                                                kViscTX * kViscTY, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, visc_tile_kernel<TX, TY, 3, PREC>, TX * TY, 0);
   *ctas_per_sm = occ < 1 ? 1 : occ;
   return e;
 }
