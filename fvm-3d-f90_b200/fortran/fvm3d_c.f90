@@ -25,7 +25,7 @@ module fvm3d_c
   public :: fvm_config_t
   public :: fvm_config_default, fvm_abi_version, fvm_create, fvm_destroy
   public :: fvm_add_block, fvm_set_boundary, fvm_connect
-  public :: fvm_set_state, fvm_get_state, fvm_get_primitive, fvm_get_rhs
+  public :: fvm_set_state, fvm_get_state, fvm_set_states, fvm_get_states, fvm_get_primitive, fvm_get_rhs
   public :: fvm_step, fvm_run, fvm_get_time, fvm_last_error
   public :: fvm_residual_norms
   public :: FVM_OK, FVM_BC_TRANSMISSIVE, FVM_BC_PERIODIC, FVM_BC_CONNECTED
@@ -117,6 +117,24 @@ module fvm3d_c
       integer(c_int), value :: blk
       real(c_double), intent(out) :: q(*)
     end function fvm_get_state
+
+    ! several blocks in one call: blk(1:n) block ids, q(1:n) = c_loc of each
+    ! block's get_q() array; the copies of consecutive blocks overlap
+    integer(c_int) function fvm_set_states(ctx, n, blk, q) bind(c, name="fvm_set_states")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      integer(c_int), intent(in) :: blk(*)
+      type(c_ptr), intent(in) :: q(*)
+    end function fvm_set_states
+
+    integer(c_int) function fvm_get_states(ctx, n, blk, q) bind(c, name="fvm_get_states")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      integer(c_int), intent(in) :: blk(*)
+      type(c_ptr), intent(in) :: q(*)
+    end function fvm_get_states
 
     integer(c_int) function fvm_get_primitive(ctx, blk, p) bind(c, name="fvm_get_primitive")
       import :: c_int, c_ptr, c_double
