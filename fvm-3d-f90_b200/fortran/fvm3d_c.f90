@@ -27,7 +27,7 @@ module fvm3d_c
   public :: fvm_add_block, fvm_set_boundary, fvm_connect
   public :: fvm_set_state, fvm_get_state, fvm_set_states, fvm_get_states, fvm_get_primitive, fvm_get_rhs
   public :: fvm_step, fvm_run, fvm_get_time, fvm_last_error
-  public :: fvm_residual_norms
+  public :: fvm_residual_norms, fvm_residual_norms_noalloc
   public :: FVM_OK, FVM_BC_TRANSMISSIVE, FVM_BC_PERIODIC, FVM_BC_CONNECTED
   public :: FVM_DT_FIXED, FVM_DT_CFL, FVM_DT_CFL_LOCAL
   public :: FVM_PREC_FP64_EXACT, FVM_PREC_FP64, FVM_PREC_FP32_FLUX
@@ -188,6 +188,15 @@ module fvm3d_c
       type(c_ptr), value :: rhs_dev, res_dev, stream
       integer(c_int64_t), intent(in) :: nvert(3)
     end function fvm_residual_norms
+
+    ! the same without any device allocation, for hosts whose GPU memory all
+    ! belongs to their own pool (limits in include/fvm3d.h)
+    integer(c_int) function fvm_residual_norms_noalloc(rhs_dev, nvert, res_dev, stream) &
+        bind(c, name="fvm_residual_norms_noalloc")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: rhs_dev, res_dev, stream
+      integer(c_int64_t), intent(in) :: nvert(3)
+    end function fvm_residual_norms_noalloc
 
   end interface
 
