@@ -81,3 +81,24 @@ def test_c_host_matches_python_bindings(tmp_path):
         assert t == runs[pulse]["t"]
         assert np.array_equal(ra, runs[pulse]["res"])
         assert np.array_equal(got, runs[pulse]["final"])
+
+
+def test_fortran_module_binds_header_functions():
+    # every bind(c) interface of the Fortran module names a function of
+    # include/fvm3d.h and has the C prototype's number of arguments (no
+    # Fortran compiler here, so the module is checked against the header)
+    import re
+
+    f90 = open(os.path.join(ROOT, "fvm-3d-f90_b200", "fortran", "fvm3d_c.f90")).read()
+    hdr = open(os.path.join(ROOT, "include", "fvm3d.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    protos = {m.group(1): m.group(2) for m in re.finditer(r"\bint\s+(fvm_\w+)\s*\(([^)]*)\)\s*;", hdr)}
+    binds = re.findall(r"function\s+(\w+)\s*\(([^)]*)\)\s*&?\s*(?:\n\s*)?bind\(c,\s*name=\"(\w+)\"\)", f90)
+    assert len(binds) >= 15
+    for fname, fargs, cname in binds:
+        assert fname == cname
+        assert cname in protos, cname
+        n_f = len([a for a in fargs.split(",") if a.strip()])
+        c_args = protos[cname].strip()
+        n_c = 0 if c_args in ("", "void") else len(c_args.split(","))
+        assert n_f == n_c, (cname, n_f, n_c)
