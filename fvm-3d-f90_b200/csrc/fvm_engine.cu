@@ -94,10 +94,7 @@ Engine::~Engine() {
 }
 
 void Engine::release() {
-  if (gexec_) cudaGraphExecDestroy(gexec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  gexec_ = nullptr;
-  graph_ = nullptr;
+  destroy_graphs();
   // roles beyond nroles_ alias role A: free each allocation once
   for (int r = 0; r < NROLE; ++r) {
     bool alias = false;
@@ -628,10 +625,7 @@ int Engine::layout() {
 }
 
 int Engine::plan() {
-  if (gexec_) cudaGraphExecDestroy(gexec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  gexec_ = nullptr;
-  graph_ = nullptr;
+  destroy_graphs();
   if (!laid_out_) {
     int rc = layout();
     if (rc) return rc;
@@ -1115,11 +1109,34 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
   return FVM_OK;
 }
 
-int Engine::build_graph() {
+void Engine::destroy_graphs() {
   if (gexec_) cudaGraphExecDestroy(gexec_);
   if (graph_) cudaGraphDestroy(graph_);
+  if (gexecm_) cudaGraphExecDestroy(gexecm_);
+  if (graphm_) cudaGraphDestroy(graphm_);
   gexec_ = nullptr;
   graph_ = nullptr;
+  gexecm_ = nullptr;
+  graphm_ = nullptr;
+}
+
+// nsteps steps: runs of kMultiSteps from the multi-step graph, the rest one
+// by one.
+cudaError_t Engine::launch_steps(int nsteps) {
+  int n = nsteps;
+  for (; gexecm_ && n >= kMultiSteps; n -= kMultiSteps) {
+    cudaError_t e = cudaGraphLaunch(gexecm_, stream);
+    if (e != cudaSuccess) return e;
+  }
+  for (; n > 0; --n) {
+    cudaError_t e = cudaGraphLaunch(gexec_, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+int Engine::build_graph() {
+  destroy_graphs();
   while (side_.size() < groups.size()) {
     cudaStream_t st;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -1144,6 +1161,19 @@ int Engine::build_graph() {
   graph_ = g;
   CK(cudaGraphInstantiate(&gexec_, graph_, 0));
   kernel_launches_per_step = launches;
+  // the same step kMultiSteps times in one graph
+  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  rc = 0;
+  for (int i = 0; i < kMultiSteps && rc == 0; ++i) rc = enqueue_step(nullptr, 0, nullptr, nullptr);
+  g = nullptr;
+  e2 = cudaStreamEndCapture(stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+  graphm_ = g;
+  CK(cudaGraphInstantiate(&gexecm_, graphm_, 0));
   return FVM_OK;
 }
 
@@ -1361,7 +1391,7 @@ int Engine::step(int nsteps) {
     int rc = prepare();
     if (rc) return rc;
   }
-  for (int i = 0; i < nsteps; ++i) CK(cudaGraphLaunch(gexec_, stream));
+  CK(launch_steps(nsteps));
   return FVM_OK;
 }
 
@@ -1395,7 +1425,7 @@ int Engine::time_stage(int reps, float* ms) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   CK(cudaEventRecord(e0, stream));
-  for (int i = 0; i < reps; ++i) CK(cudaGraphLaunch(gexec_, stream));
+  CK(launch_steps(reps));
   CK(cudaEventRecord(e1, stream));
   CK(cudaEventSynchronize(e1));
   CK(cudaEventElapsedTime(ms, e0, e1));

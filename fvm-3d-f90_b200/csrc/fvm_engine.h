@@ -180,6 +180,13 @@ class Engine {
   int ensure_xfer();
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t gexec_ = nullptr;
+  // kMultiSteps steps in one graph: runs of steps cost one launch per
+  // kMultiSteps (what decides the step rate of small cases)
+  static constexpr int kMultiSteps = 8;
+  cudaGraph_t graphm_ = nullptr;
+  cudaGraphExec_t gexecm_ = nullptr;
+  void destroy_graphs();
+  cudaError_t launch_steps(int nsteps);
   std::vector<cudaStream_t> side_;  // fork streams for parallel group launches
   std::vector<cudaEvent_t> fork_ev_;
   std::vector<DevBlock> h_dblocks_;
