@@ -82,7 +82,7 @@ class Dist:
 
             import torch.distributed as dist
 
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
             self.pg = dist
 
     def barrier(self):
