@@ -20,30 +20,31 @@ namespace fvm {
 // reference describes in defs_face_geom.f90:378-402 but never performs).
 // Every source is a real cell (the host resolves ghost-to-ghost chains), so
 // the pairs are independent. Each thread takes kGatherPer pairs a grid
-// apart (a warp's pairs stay consecutive) and issues all their loads before
-// any store, so the index-then-data latency chain is paid once per thread.
+// apart (a warp's pairs stay consecutive; each pair one 8-byte load of two
+// 32-bit cell offsets) and issues all their loads before any store, so the
+// index-then-data latency chain is paid once per thread.
 constexpr int kGatherPer = 4;
-__global__ void gather_kernel(double* __restrict__ base, int64_t vs, const longlong2* __restrict__ pairs,
+__global__ void gather_kernel(double* __restrict__ base, int64_t vs, const int2* __restrict__ pairs,
                               int64_t npairs) {
   const int64_t G = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += G * kGatherPer) {
-    longlong2 p[kGatherPer];
+    int2 p[kGatherPer];
 #pragma unroll
     for (int j = 0; j < kGatherPer; ++j) {
       const int64_t i = i0 + j * G;
-      p[j] = i < npairs ? pairs[i] : make_longlong2(-1, -1);
+      p[j] = i < npairs ? pairs[i] : make_int2(-1, -1);
     }
     double val[kGatherPer][5];
 #pragma unroll
     for (int j = 0; j < kGatherPer; ++j)
       if (p[j].x >= 0)
 #pragma unroll
-        for (int v = 0; v < 5; ++v) val[j][v] = base[p[j].y + v * vs];
+        for (int v = 0; v < 5; ++v) val[j][v] = base[(int64_t)p[j].y + v * vs];
 #pragma unroll
     for (int j = 0; j < kGatherPer; ++j)
       if (p[j].x >= 0)
 #pragma unroll
-        for (int v = 0; v < 5; ++v) base[p[j].x + v * vs] = val[j][v];
+        for (int v = 0; v < 5; ++v) base[(int64_t)p[j].x + v * vs] = val[j][v];
   }
 }
 
@@ -229,10 +230,10 @@ static inline int grid_for(int64_t n, int bs) {
   return (int)g;
 }
 
-cudaError_t launch_gather(double* base, int64_t vs, const int64_t* pairs, int64_t npairs, cudaStream_t s) {
+cudaError_t launch_gather(double* base, int64_t vs, const int32_t* pairs, int64_t npairs, cudaStream_t s) {
   if (npairs == 0) return cudaSuccess;
   const int64_t threads = (npairs + kGatherPer - 1) / kGatherPer;
-  gather_kernel<<<grid_for(threads, 256), 256, 0, s>>>(base, vs, reinterpret_cast<const longlong2*>(pairs), npairs);
+  gather_kernel<<<grid_for(threads, 256), 256, 0, s>>>(base, vs, reinterpret_cast<const int2*>(pairs), npairs);
   return cudaGetLastError();
 }
 

@@ -8,7 +8,7 @@
 
 namespace fvm {
 
-cudaError_t launch_gather(double* base, int64_t vs, const int64_t* pairs, int64_t npairs, cudaStream_t s);
+cudaError_t launch_gather(double* base, int64_t vs, const int32_t* pairs, int64_t npairs, cudaStream_t s);
 cudaError_t launch_unpack(double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, const double* src,
                           cudaStream_t s);
 cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, double* dst,

@@ -971,7 +971,11 @@ int Engine::plan() {
   CK(cudaMalloc(&d_case_blk_, sizeof(int) * std::max<size_t>(1, case_blk.size())));
   CK(cudaMalloc(&d_tasks_, sizeof(Task) * std::max<size_t>(1, tasks.size())));
   CK(cudaMalloc(&d_partials_, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size())));
-  CK(cudaMalloc(&d_pairs_, sizeof(int64_t) * std::max<size_t>(2, pairs.size())));
+  // cell offsets within a role slab stay below 2^31 (a slab of 2^31 cells
+  // would take 344 GB in the 4 roles, twice the HBM): 8 bytes per pair
+  if (cap_ >= ((int64_t)1 << 31)) return fail(FVM_ERR_INVALID, "arena too large for 32-bit ghost offsets");
+  std::vector<int32_t> pairs32(pairs.begin(), pairs.end());
+  CK(cudaMalloc(&d_pairs_, sizeof(int32_t) * std::max<size_t>(2, pairs32.size())));
   ncounters_ = max_stages_ * (int)groups.size();
   CK(cudaMalloc(&d_counters_, sizeof(int) * std::max(1, ncounters_)));
   CK(cudaMalloc(&d_casemax_, sizeof(unsigned long long) * cases.size()));
@@ -982,7 +986,7 @@ int Engine::plan() {
   if (!tasks.empty())
     CK(cudaMemcpyAsync(d_tasks_, tasks.data(), sizeof(Task) * tasks.size(), cudaMemcpyHostToDevice, stream));
   if (!pairs.empty())
-    CK(cudaMemcpyAsync(d_pairs_, pairs.data(), sizeof(int64_t) * pairs.size(), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_pairs_, pairs32.data(), sizeof(int32_t) * pairs32.size(), cudaMemcpyHostToDevice, stream));
   CK(cudaMemsetAsync(d_counters_, 0, sizeof(int) * std::max(1, ncounters_), stream));
   CK(cudaMemsetAsync(d_partials_, 0, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size()), stream));
 

@@ -160,7 +160,7 @@ class Engine {
   int state_cap_ = 0;
   Task* d_tasks_ = nullptr;
   double* d_partials_ = nullptr;
-  int64_t* d_pairs_ = nullptr;
+  int32_t* d_pairs_ = nullptr;       // (dst, src) cell offsets within a role slab
   int* d_counters_ = nullptr;
   int ncounters_ = 0;
   // viscous task lists in d_tasks_, index precision * 2 + (3D ? 0 : 1)
