@@ -205,6 +205,48 @@ def test_fp32_flux_vortex_l1():
     assert err <= 1e-6, err
 
 
+def _oracle_and_forms(case, steps):
+    o = case.apply(orc.Oracle(case.config()))
+    o.step(steps)
+    out = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32", abi.PREC_FP32_FLUX)):
+        g = case.apply(Solver(case.config(precision=prec)))
+        g.step(steps)
+        out[name] = [g.get_state(b) for b in range(len(case.blocks))]
+        g.close()
+    return [o.get_state(b) for b in range(len(case.blocks))], out
+
+
+FAST_SCHEMES = [(r, f, abi.COMPAT_REFERENCE) for r, f in RECON_FLUX] + \
+    [(abi.RECON_WENO, abi.FLUX_AUSM, abi.COMPAT_TEXTBOOK), (abi.RECON_WENO, abi.FLUX_ROE, abi.COMPAT_TEXTBOOK)]
+
+
+@pytest.mark.parametrize("recon,flux,compat", FAST_SCHEMES)
+def test_fast_forms_every_scheme_3d(recon, flux, compat):
+    # every reconstruction x flux kernel of the FP64 and FP32-flux forms on
+    # the smooth 8-block vortex (Van Albada: no limiter branch to flip on a
+    # rounding difference), SSP-RK3, against the exact oracle
+    c = cases.isentropic_vortex(N=24, layout="blocks8", reconstruct=recon, flux_split=flux, compat=compat,
+                                rk_stages=3, limiter=abi.LIMITER_VANALBADA, kappa=1.0 / 3.0)
+    ref, got = _oracle_and_forms(c, 5)
+    for b in range(8):
+        assert np.abs(got["fp64"][b] - ref[b]).max() <= 1e-11 * np.abs(ref[b]).max(), f"fp64 block {b}"
+    err32 = np.mean([np.abs(got["fp32"][b][0] - ref[b][0]).mean() for b in range(8)])
+    assert err32 <= 1e-6, err32
+
+
+@pytest.mark.parametrize("recon,flux", [(abi.RECON_MUSCL, abi.FLUX_ROE), (abi.RECON_WENO, abi.FLUX_AUSM),
+                                        (abi.RECON_SIMPLE, abi.FLUX_VANLEER)])
+def test_fast_forms_2d(recon, flux):
+    # the 2D kernels of the FP64 and FP32-flux forms (per-thread staged
+    # planes, no tensor copies) on the four-quadrant Riemann problem
+    c = cases.riemann2d(n=40, seed=2, reconstruct=recon, flux_split=flux, limiter=abi.LIMITER_VANALBADA,
+                        kappa=1.0 / 3.0, dt=1e-3)
+    ref, got = _oracle_and_forms(c, 3)
+    assert np.abs(got["fp64"][0][0] - ref[0][0]).mean() <= 1e-10
+    assert np.abs(got["fp32"][0][0] - ref[0][0]).mean() <= 1e-5
+
+
 def test_primitive_download():
     c = cases.riemann2d(n=20, seed=0, dt=1e-3)
     g, o, _, _ = run_both(c, 2)
