@@ -119,7 +119,7 @@ class Clocks:
 
             nv.nvmlInit()
             self.nv = nv
-            self.h = nv.nvmlDeviceGetHandleByIndex(index)
+            self.h, self.found_by = self._handle(nv, index)
             self.max_sm = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
             self.ok = True
         except Exception as e:  # noqa: BLE001
@@ -128,6 +128,24 @@ class Clocks:
         self.stop_flag = False
         self.th = threading.Thread(target=self._run, daemon=True)
         self.th.start()
+
+    @staticmethod
+    def _handle(nv, index):
+        """The NVML device of CUDA device `index` of this process: NVML numbers
+        the machine's GPUs and ignores CUDA_VISIBLE_DEVICES, so the device is
+        matched by UUID, else by PCI bus id; physical index 0 only as a last
+        resort (said so in the record)."""
+        try:
+            import torch
+
+            p = torch.cuda.get_device_properties(index)
+            try:
+                return nv.nvmlDeviceGetHandleByUUID(("GPU-" + str(p.uuid)).encode()), "uuid"
+            except Exception:  # noqa: BLE001
+                bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+                return nv.nvmlDeviceGetHandleByPciBusId(bus.encode()), "pci bus id"
+        except Exception:  # noqa: BLE001
+            return nv.nvmlDeviceGetHandleByIndex(0), "nvml index 0 (no match)"
 
     def _run(self):
         # SM clock and reasons every millisecond (the timed region of a short
@@ -159,7 +177,8 @@ class Clocks:
         reasons = sorted({n for r in self.rows for n, bit in self.REASONS.items() if r[1] & bit})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_sm,
                 "power_w_max": max((r[2] for r in self.rows), default=None), "samples": len(self.rows),
-                "reasons": reasons, "source": "NVML, 1 ms sampling during the timed steps"}
+                "reasons": reasons, "source": "NVML, 1 ms sampling during the timed steps",
+                "device_matched_by": self.found_by}
 
 
 def peaks() -> dict:
