@@ -26,6 +26,8 @@ namespace fvm {
 constexpr int kGatherPer = 4;
 __global__ void gather_kernel(double* __restrict__ base, int64_t vs, const int2* __restrict__ pairs,
                               int64_t npairs) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t G = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += G * kGatherPer) {
     int2 p[kGatherPer];
@@ -139,6 +141,8 @@ __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, co
   // accumulates them (class_iteration.f90:195-259)
   constexpr int NW = 8;
   __shared__ double red[NW][6];
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const DevCase& C = cases[c];
   if (c == 0)
@@ -230,11 +234,12 @@ static inline int grid_for(int64_t n, int bs) {
   return (int)g;
 }
 
-cudaError_t launch_gather(double* base, int64_t vs, const int32_t* pairs, int64_t npairs, cudaStream_t s) {
+cudaError_t launch_gather(double* base, int64_t vs, const int32_t* pairs, int64_t npairs, cudaStream_t s,
+                          bool pdl) {
   if (npairs == 0) return cudaSuccess;
   const int64_t threads = (npairs + kGatherPer - 1) / kGatherPer;
-  gather_kernel<<<grid_for(threads, 256), 256, 0, s>>>(base, vs, reinterpret_cast<const int2*>(pairs), npairs);
-  return cudaGetLastError();
+  LaunchCfg L(dim3(grid_for(threads, 256)), dim3(256), 0, s, pdl);
+  return cudaLaunchKernelEx(&L.cfg, gather_kernel, base, vs, reinterpret_cast<const int2*>(pairs), npairs);
 }
 
 cudaError_t launch_unpack(double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, const double* src,
@@ -263,9 +268,10 @@ cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* c
 }
 
 cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
-                            int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s) {
-  finalize_kernel<<<ncases, 256, 0, s>>>(blocks, cases, case_blk, st, partials, counters, ncounters);
-  return cudaGetLastError();
+                            int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s,
+                            bool pdl) {
+  LaunchCfg L(dim3(ncases), dim3(256), 0, s, pdl);
+  return cudaLaunchKernelEx(&L.cfg, finalize_kernel, blocks, cases, case_blk, st, partials, counters, ncounters);
 }
 
 cudaError_t visc_occupancy(int prec, int* ctas_per_sm) {
@@ -288,9 +294,9 @@ cudaError_t launch_fast_math_probe(const double* x, int64_t n, double* r, double
 }
 
 cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
-                        int prec, int role, cudaStream_t s) {
-  if (prec == PREC_EXACT) return launch_visc_prec<PREC_EXACT>(blocks, cases, tasks, ntasks, idim, role, s);
-  return launch_visc_fast(blocks, cases, tasks, ntasks, idim, prec, role, s);
+                        int prec, int role, cudaStream_t s, bool pdl) {
+  if (prec == PREC_EXACT) return launch_visc_prec<PREC_EXACT>(blocks, cases, tasks, ntasks, idim, role, s, pdl);
+  return launch_visc_fast(blocks, cases, tasks, ntasks, idim, prec, role, s, pdl);
 }
 
 }  // namespace fvm

@@ -8,7 +8,30 @@
 
 namespace fvm {
 
-cudaError_t launch_gather(double* base, int64_t vs, const int32_t* pairs, int64_t npairs, cudaStream_t s);
+// A launch configuration, with programmatic stream serialization when pdl is
+// set (the kernel must call pdl_wait() first). Used in place: cfg.attrs
+// points into the object.
+struct LaunchCfg {
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1]{};
+  LaunchCfg(dim3 grid, dim3 block, size_t smem, cudaStream_t s, bool pdl) {
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+  }
+  LaunchCfg(const LaunchCfg&) = delete;
+  LaunchCfg& operator=(const LaunchCfg&) = delete;
+};
+
+// gather, finalize and visc take pdl: launch with programmatic stream
+// serialization (inside the step graphs).
+cudaError_t launch_gather(double* base, int64_t vs, const int32_t* pairs, int64_t npairs, cudaStream_t s,
+                          bool pdl = false);
 cudaError_t launch_unpack(double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, const double* src,
                           cudaStream_t s);
 cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int ni, int nj, int nk, double* dst,
@@ -16,7 +39,8 @@ cudaError_t launch_pack(const double* role_blk, int64_t vs, int sy, int sz, int 
 cudaError_t launch_init_dt(const DevBlock* blocks, int nblocks, const DevCase* cases, DevCaseState* st, int ncases,
                            unsigned long long* case_max, const int* mask, int role, cudaStream_t s);
 cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
-                            int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s);
+                            int ncases, const double* partials, int* counters, int ncounters, cudaStream_t s,
+                            bool pdl = false);
 // Viscous contribution of the Navier-Stokes blocks: one CTA per task of a
 // viscous task list (column tiles over z ranges), all of dimension idim and
 // precision form prec (PREC_*). The tile is 16 x 8 for the FP64 forms and
@@ -27,10 +51,10 @@ cudaError_t launch_finalize(const DevBlock* blocks, const DevCase* cases, const 
 constexpr int visc_tx(int prec) { return prec == 2 ? 32 : 16; }
 constexpr int visc_ty(int prec) { return prec == 2 ? 4 : 8; }
 cudaError_t launch_visc(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
-                        int prec, int role, cudaStream_t s);
+                        int prec, int role, cudaStream_t s, bool pdl = false);
 cudaError_t visc_occupancy(int prec, int* ctas_per_sm);
 cudaError_t launch_visc_fast(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
-                             int prec, int role, cudaStream_t s);
+                             int prec, int role, cudaStream_t s, bool pdl);
 cudaError_t visc_occupancy_fast(int prec, int* ctas_per_sm);
 // rcp_ / rsqrt_ of the non-exact FP64 forms over x[0..n) (device arrays).
 cudaError_t launch_fast_math_probe(const double* x, int64_t n, double* r, double* rs, cudaStream_t s);

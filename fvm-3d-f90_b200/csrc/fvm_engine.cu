@@ -1044,6 +1044,10 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
   // groups run as parallel branches of the captured graph (fork / join on
   // side streams); the profiled path launches them in sequence to time each
   const bool fork = (evs == nullptr) && groups.size() > 1;
+  // a single-group step graph chains its kernels by programmatic dependent
+  // launch: each launch's CTAs are scheduled while its predecessor drains
+  // (every step kernel begins with pdl_wait)
+  const bool pdl = (evs == nullptr) && !fork;
   int n = 0;
   auto mark = [&](int kind) -> cudaError_t {
     if (evs && n < nev) {
@@ -1063,7 +1067,7 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
     for (int li = 0; li < 6; ++li) {
       if (vlist_n_[li] == 0) continue;
       CK(launch_visc(d_blocks_, d_cases_, d_tasks_ + vlist_off_[li], vlist_n_[li], li % 2 == 0 ? 3 : 2, li / 2,
-                     rin, stream));
+                     rin, stream, pdl));
       CK(mark(3));
     }
     if (fork) CK(cudaEventRecord(fork_ev_[ev_i], stream));
@@ -1093,7 +1097,8 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
         st = side_[g];
         CK(cudaStreamWaitEvent(st, fork_ev_[fork_ev], 0));
       }
-      CK(cudaLaunchKernel(G.k.fn, dim3(G.grid), dim3(G.k.threads), args, G.k.smem, st));
+      LaunchCfg L(dim3(G.grid), dim3(G.k.threads), G.k.smem, st, pdl);
+      CK(cudaLaunchKernelExC(&L.cfg, G.k.fn, args));
       if (fork) {
         CK(cudaEventRecord(fork_ev_[ev_i], st));
         CK(cudaStreamWaitEvent(stream, fork_ev_[ev_i], 0));
@@ -1102,12 +1107,12 @@ int Engine::enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch) {
       CK(mark(1));
     }
     if (npairs > 0) {
-      CK(launch_gather(role_[rout], cap_, d_pairs_, npairs, stream));
+      CK(launch_gather(role_[rout], cap_, d_pairs_, npairs, stream, pdl));
       CK(mark(2));
     }
   }
   CK(launch_finalize(d_blocks_, d_cases_, d_case_blk_, d_state_, (int)cases.size(), d_partials_, d_counters_,
-                     ncounters_, stream));
+                     ncounters_, stream, pdl));
   CK(mark(4));
   if (nlaunch) *nlaunch = n;
   return FVM_OK;

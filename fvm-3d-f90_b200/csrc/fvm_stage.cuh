@@ -346,6 +346,9 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
     }
     __syncthreads();
   }
+  // no early pdl_trigger here: the gather launched behind this kernel would
+  // place its CTAs on the first SMs to free up and run unbalanced
+  pdl_wait();
 
   for (;;) {
     if (tid == 0) s_task = atomicAdd(a.counter, 1);

@@ -95,4 +95,20 @@ struct StageArgs {
   int32_t drop_copies;         // test of the timeout path: arm the barrier, skip the copy
 };
 
+// Programmatic dependent launch. Inside the step graphs the kernels of a time
+// step are launched with programmatic stream serialization, so the CTAs of a
+// launch are scheduled while the one before it drains. Every kernel of that
+// chain calls pdl_wait() before it touches global memory: it returns once the
+// preceding kernel has completed and its writes are visible (at once for a
+// kernel launched without the attribute). As every kernel of the chain waits,
+// the completion of one implies that of all before it. pdl_trigger() lets the
+// next launch be scheduled once every CTA of this one has started; it orders
+// no memory. Only the short gather and finalize kernels trigger early: a
+// launch scheduled behind a long kernel's tail places its CTAs on the few SMs
+// free at that moment (up to 8 gather CTAs per SM) and runs unbalanced.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+#endif
+
 }  // namespace fvm

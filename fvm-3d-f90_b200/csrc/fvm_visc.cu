@@ -5,9 +5,9 @@
 namespace fvm {
 
 cudaError_t launch_visc_fast(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
-                             int prec, int role, cudaStream_t s) {
-  if (prec == PREC_FP32) return launch_visc_prec<PREC_FP32>(blocks, cases, tasks, ntasks, idim, role, s);
-  return launch_visc_prec<PREC_FP64>(blocks, cases, tasks, ntasks, idim, role, s);
+                             int prec, int role, cudaStream_t s, bool pdl) {
+  if (prec == PREC_FP32) return launch_visc_prec<PREC_FP32>(blocks, cases, tasks, ntasks, idim, role, s, pdl);
+  return launch_visc_prec<PREC_FP64>(blocks, cases, tasks, ntasks, idim, role, s, pdl);
 }
 
 cudaError_t visc_occupancy_fast(int prec, int* ctas_per_sm) {

@@ -370,6 +370,7 @@ __global__ void __launch_bounds__(TX* TY, ViscMinBlocks<PREC>::v)
   using PT = PrecT<PREC>;
   __shared__ __align__(16)
       unsigned char smem[ViscCfg<TX, TY, IDIM>::template Smem<(int)sizeof(typename PT::R)>::v];
+  pdl_wait();  // no early trigger (see stage_kernel)
   const Task T = tasks[blockIdx.x];
   const DevBlock& B = blocks[T.blk];
   visc_tile_body<TX, TY, IDIM, PT::ex, typename PT::R>(B, cases[B.case_id], T, role, smem);
@@ -377,14 +378,12 @@ __global__ void __launch_bounds__(TX* TY, ViscMinBlocks<PREC>::v)
 
 template <int PREC>
 cudaError_t launch_visc_prec(const DevBlock* blocks, const DevCase* cases, const Task* tasks, int ntasks, int idim,
-                             int role, cudaStream_t s) {
+                             int role, cudaStream_t s, bool pdl) {
   constexpr int TX = visc_tx(PREC), TY = visc_ty(PREC);
   if (ntasks == 0) return cudaSuccess;
-  if (idim == 3)
-    visc_tile_kernel<TX, TY, 3, PREC><<<ntasks, TX * TY, 0, s>>>(blocks, cases, tasks, role);
-  else
-    visc_tile_kernel<TX, TY, 2, PREC><<<ntasks, TX * TY, 0, s>>>(blocks, cases, tasks, role);
-  return cudaGetLastError();
+  LaunchCfg L(dim3(ntasks), dim3(TX * TY), 0, s, pdl);
+  if (idim == 3) return cudaLaunchKernelEx(&L.cfg, visc_tile_kernel<TX, TY, 3, PREC>, blocks, cases, tasks, role);
+  return cudaLaunchKernelEx(&L.cfg, visc_tile_kernel<TX, TY, 2, PREC>, blocks, cases, tasks, role);
 }
 
 template <int PREC>
