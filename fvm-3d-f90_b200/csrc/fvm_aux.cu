@@ -137,10 +137,13 @@ __global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const uns
 __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                                 const double* partials, int* counters, int ncounters) {
   // one warp per block reduces its task partials (lanes stride the tasks,
-  // then a butterfly); thread 0 folds the blocks in order, as the reference
-  // accumulates them (class_iteration.f90:195-259)
+  // then a butterfly) and its lane 0 turns the sums into the block's squared
+  // norms; thread 0 folds the blocks in order, as the reference accumulates
+  // them (class_iteration.f90:195-259). The six folds are independent
+  // chains, so a block costs thread 0 one square root of latency.
   constexpr int NW = 8;
   __shared__ double red[NW][6];
+  __shared__ double redm[NW];
   pdl_wait();
   pdl_trigger();
   const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -186,25 +189,24 @@ __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, co
         m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
       }
       if (lane == 0) {
+        const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
+        double res2_t = 0.0;
 #pragma unroll
-        for (int v = 0; v < 5; ++v) red[warp][v] = s[v];
-        red[warp][5] = m;
+        for (int v = 0; v < 5; ++v) {
+          const double r2 = s[v] / npt;
+          red[warp][v] = r2;
+          res2_t = res2_t + r2;
+        }
+        red[warp][5] = res2_t / 5.0;
+        redm[warp] = m;
       }
     }
     __syncthreads();
     if (tid == 0) {
       for (int w = 0; w < NW && b0 + w < C.nblocks; ++w) {
-        const DevBlock& B = blocks[case_blk[C.block0 + b0 + w]];
-        const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
-        double res2[5], res2_t = 0.0;
-        for (int v = 0; v < 5; ++v) {
-          res2[v] = red[w][v] / npt;
-          res2_t = res2_t + res2[v];
-        }
-        res2_t = res2_t / 5.0;
-        for (int v = 0; v < 5; ++v) res[v] = sqrt(res[v] * res[v] + res2[v]);
-        res[5] = sqrt(res[5] * res[5] + res2_t);
-        wmax = fmax(wmax, red[w][5]);
+#pragma unroll
+        for (int v = 0; v < 6; ++v) res[v] = sqrt(res[v] * res[v] + red[w][v]);
+        wmax = fmax(wmax, redm[w]);
       }
     }
     __syncthreads();
