@@ -23,8 +23,9 @@ namespace fvm {
 // apart (a warp's pairs stay consecutive; each pair one 8-byte load of two
 // 32-bit cell offsets) and issues all their loads before any store, so the
 // index-then-data latency chain is paid once per thread. Capped at 64
-// registers, four 256-thread CTAs fit on an SM, so the bench workload's 576
-// CTAs run as one wave (at 68 registers, three per SM: 444 + 132).
+// registers, four 256-thread CTAs fit on an SM, so the 576 CTAs of the 128^3
+// vortex in 8 blocks (583 K ghost cells) run as one wave (at 68 registers,
+// three per SM: 444 + 132).
 constexpr int kGatherPer = 4;
 __global__ void __launch_bounds__(256, 4) gather_kernel(double* __restrict__ base, int64_t vs, const int2* __restrict__ pairs,
                               int64_t npairs) {
