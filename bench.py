@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--tile", type=int, default=None, help="fixed tile index (skips the autotuner)")
     ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk with --tile")
+    ap.add_argument("--tail-split", type=int, default=1, help="fixed tail split with --tile (1 = none)")
     ap.add_argument("--forms", default="fp32,fp64,exact",
                     help="comma list of arms: fp32 (headline), fp64, exact")
     ap.add_argument("--only", choices=["tgv", "riemann2d", "accuracy"], default=None,
@@ -202,26 +203,27 @@ def product(args, dist: Dist):
     stages = 4
     nblk = len(case.blocks)
 
-    def fresh(prec, tile=None, z=None):
+    def fresh(prec, tile=None, z=None, sp=1):
         s = Solver(case.config(precision=prec))
         case.apply(s, states=False)
         if tile is not None:
             tuning.set_tuning(s, 0, tile, z)
+            tuning.set_tail_split(s, 0, sp)
         for b, q in enumerate(case.states):
             s.set_state(b, q)
         return s
 
     def tune(prec):
         if args.tile is not None:
-            return args.tile, args.zchunk
+            return args.tile, args.zchunk, args.tail_split
         s = fresh(prec)
-        t, z, ms = tuning.autotune(s, ncells, use_cache=False, reps=2)
+        t, z, ms, sp = tuning.autotune(s, ncells, use_cache=False, reps=2)
         s.close()
-        return t, z
+        return t, z, sp
 
     def timed(prec):
-        tile, z = tune(prec)
-        s = fresh(prec, tile, z)
+        tile, z, sp = tune(prec)
+        s = fresh(prec, tile, z, sp)
         s.step(args.warmup)
         dist.barrier()
         clk = Clocks(0) if dist.rank == 0 else None
@@ -232,7 +234,7 @@ def product(args, dist: Dist):
         for _ in range(3):
             prof.append(tuning.profile_step(s))
         launches = tuning.launches_per_step(s)
-        return s, ms_max, clocks, prof, launches, (tile, z)
+        return s, ms_max, clocks, prof, launches, (tile, z, sp)
 
     out = {}
     forms = set(args.forms.split(","))
@@ -284,16 +286,18 @@ def product(args, dist: Dist):
     out["gpu_launches"] = launches * args.steps
     if s64 is not None:
         out["fp64_plain"] = {"value": gcs(ms64), "ms_per_step": ms64, "roofline": roof(prof64),
-                             "tile_zchunk": tz64}
+                             "tile_zchunk": tz64[:2], "tail_split": tz64[2]}
         # L1 density difference of the FP32-flux form against FP64 after the same steps
         out["l1_density_err_vs_fp64"] = l1rho(s32, s64)
     if sx is not None:
-        out["fp64_exact"] = {"value": gcs(msx), "ms_per_step": msx, "roofline": roof(profx), "tile_zchunk": tzx}
+        out["fp64_exact"] = {"value": gcs(msx), "ms_per_step": msx, "roofline": roof(profx), "tile_zchunk": tzx[:2],
+                             "tail_split": tzx[2]}
         if s64 is not None:
             out["fp64_plain"]["l1_density_vs_fp64_exact"] = l1rho(s64, sx)
         else:
             out["l1_density_err_vs_fp64"] = l1rho(s32, sx)
-    out["tile_zchunk"] = tz32
+    out["tile_zchunk"] = tz32[:2]
+    out["tail_split"] = tz32[2]
     out["profile_ms"] = {k: round(sum(ms for p in prof32 for kk, ms in p if kk == k) / len(prof32), 4)
                          for k in ("stage", "gather", "finalize")}
     for x in (sx, s64):

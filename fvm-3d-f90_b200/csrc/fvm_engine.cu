@@ -425,6 +425,15 @@ int Engine::set_tuning(int case_id, int tile, int zchunk) {
   return FVM_OK;
 }
 
+int Engine::set_tail_split(int case_id, int split) {
+  if (!live_case(case_id)) return fail(FVM_ERR_INVALID, "bad case id");
+  if (split < 1 || split > 8) return fail(FVM_ERR_INVALID, "bad tail split");
+  if (cases[case_id].tail_split == split) return FVM_OK;
+  cases[case_id].tail_split = split;
+  invalidate();
+  return FVM_OK;
+}
+
 // ---------------------------------------------------------------- arena
 int Engine::alloc_range(int64_t size, int64_t* off) {
   for (size_t i = 0; i < free_.size(); ++i) {
@@ -734,6 +743,7 @@ int Engine::plan() {
         }
       }
       std::vector<int64_t> z0s;
+      std::vector<Task> ct;
       for (int bi : hc.blocks) {
         const HBlock& b = blocks[bi];
         if (G.dim == 3)
@@ -750,9 +760,37 @@ int Engine::plan() {
               t.z0 = (int)z0s[c];
               t.z1 = (int)z0s[c + 1];
               t.slot = 0;
-              gt.push_back(t);
+              ct.push_back(t);
             }
       }
+      // Tail split: when the case's tasks fill the queue's slots (resident
+      // CTAs) k times and r more, its r shortest tasks are cut along z into
+      // tail_split pieces, so the last, partial round of the queue runs on
+      // more CTAs for a shorter time (each piece warms up its own z window).
+      // It depends on the case and the kernel's slot count only, so a case
+      // is tiled alike alone and batched.
+      if (G.dim == 3 && hc.tail_split > 1 && (int64_t)ct.size() > G.grid) {
+        std::stable_sort(ct.begin(), ct.end(),
+                         [](const Task& a, const Task& b) { return (a.z1 - a.z0) > (b.z1 - b.z0); });
+        const size_t r = ct.size() % (size_t)G.grid;
+        std::vector<Task> pieces;
+        for (size_t i = ct.size() - r; i < ct.size(); ++i) {
+          const Task& t = ct[i];
+          const int n = t.z1 - t.z0;
+          const int sp = std::min(hc.tail_split, n / 2);  // pieces of at least 2 planes
+          for (int q = 0; q < std::max(sp, 1); ++q) {
+            Task u = t;
+            if (sp > 1) {
+              u.z0 = t.z0 + (int)((int64_t)n * q / sp);
+              u.z1 = t.z0 + (int)((int64_t)n * (q + 1) / sp);
+            }
+            pieces.push_back(u);
+          }
+        }
+        ct.resize(ct.size() - r);
+        ct.insert(ct.end(), pieces.begin(), pieces.end());
+      }
+      gt.insert(gt.end(), ct.begin(), ct.end());
     }
     std::stable_sort(gt.begin(), gt.end(), [](const Task& a, const Task& b) { return (a.z1 - a.z0) > (b.z1 - b.z0); });
     tasks.insert(tasks.end(), gt.begin(), gt.end());
@@ -1676,6 +1714,11 @@ int fvm_case_state(fvm_ctx* ctx, int case_id, double* t, double* dt, int64_t* st
 int fvm_tune_set(fvm_ctx* ctx, int case_id, int tile, int zchunk) {
   if (!ctx) return FVM_ERR_INVALID;
   return ctx->eng.set_tuning(case_id, tile, zchunk);
+}
+
+int fvm_tune_set_tail_split(fvm_ctx* ctx, int case_id, int split) {
+  if (!ctx) return FVM_ERR_INVALID;
+  return ctx->eng.set_tail_split(case_id, split);
 }
 
 int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step) {

@@ -59,6 +59,7 @@ struct HCase {
   int group = -1;
   int tile = -1;        // forced tile (autotuner result), -1 = heuristic
   int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model
+  int tail_split = 1;   // pieces each task of the last, partial queue round is cut into (1 = none)
   // cost-model choice cached per (tile, grid); depends on the case alone
   std::pair<int, int> auto_key{-1, -1};
   int64_t auto_zchunk = 0;
@@ -100,6 +101,7 @@ class Engine {
   int set_drop_copies(bool on);
   // Tuning hooks (autotuner): force tile shape / z chunk of a case.
   int set_tuning(int case_id, int tile, int zchunk);
+  int set_tail_split(int case_id, int split);
   // Mean device time of `reps` graph-launched steps (ms).
   int time_stage(int reps, float* ms);
 

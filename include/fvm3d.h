@@ -236,8 +236,13 @@ int fvm_case_state(fvm_ctx* ctx, int case_id, double* t, double* dt, int64_t* st
  * resident CTAs per SM; -1 = heuristic) and z chunk length
  * (0 = heuristic) of the fused stage kernel for case `case_id`, keeping the
  * current state; fvm_tune_time_step runs `reps` full time steps (the state
- * advances) and returns the mean device time per step in ms. */
+ * advances) and returns the mean device time per step in ms.
+ * fvm_tune_set_tail_split (3D; split 1..8, 1 = off, the default): when the
+ * case's tasks fill the stage kernel's resident CTAs k times and r more, its
+ * r shortest tasks are cut along z into `split` pieces (of at least 2
+ * planes), so the last, partial round of the work queue is shorter. */
 int fvm_tune_set(fvm_ctx* ctx, int case_id, int tile, int zchunk);
+int fvm_tune_set_tail_split(fvm_ctx* ctx, int case_id, int split);
 int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step);
 /* Profiling hooks; no counterpart in the reference. fvm_profile_step runs one
  * time step launch by launch with a CUDA event after each and returns the

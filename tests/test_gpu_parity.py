@@ -97,6 +97,33 @@ def test_tiling_does_not_change_state(tile, zchunk):
         assert np.array_equal(g.get_state(b), o.get_state(b))
 
 
+@pytest.mark.parametrize("split", [2, 4])
+def test_tail_split_does_not_change_state(split):
+    # 16x8 tiles with 4-plane z chunks on the 96^3 vortex in 8 blocks give
+    # 1728 tasks, more than the stage kernel's resident CTAs, so the work
+    # queue has a partial last round whose tasks are cut into `split` pieces
+    from fvm3d import tuning
+    from fvm3d.solver import FvmError
+
+    c = cases.isentropic_vortex(N=96, layout="blocks8")
+    o = c.apply(orc.Oracle(c.config()))
+    ro = o.step(2)
+    g = Solver(c.config())
+    c.apply(g, states=False)
+    tuning.set_tuning(g, 0, 3, 4)
+    tuning.set_tail_split(g, 0, split)
+    with pytest.raises(FvmError) as e:
+        tuning.set_tail_split(g, 0, 0)
+    assert e.value.code == 1  # FVM_ERR_INVALID
+    for b, q in enumerate(c.states):
+        g.set_state(b, q)
+    rg = g.step(2)
+    for b in range(8):
+        assert np.array_equal(g.get_state(b), o.get_state(b))
+    # the residual norms sum the same cells over a different partition
+    np.testing.assert_allclose(rg[1], ro[1], rtol=1e-12)
+
+
 @pytest.mark.parametrize("recon,flux", [(abi.RECON_MUSCL, abi.FLUX_ROE), (abi.RECON_WENO, abi.FLUX_VANLEER)])
 def test_tma_tile_rk3_exact(recon, flux):
     # the 16x8 tile (plane, z window and RK operands by tensor copies) in the
