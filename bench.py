@@ -35,7 +35,10 @@ sys.path.insert(0, PKG)
 
 METRIC = "Gcell-stage/s FP64 plain vs FP32-batched at L1 err<=1e-6; served p50/p99 latency"
 UNIT = "Gcell-stage/s"
-STAGE_TRAFFIC_FP32 = 402.10e6  # bytes per stage launch, ncu dram__bytes_read.sum + dram__bytes_write.sum
+# DRAM bytes per stage launch of the FP32 form on the 128^3 vortex (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum, mean of the 4 launches of one
+# step), by (tile index, tail split): 16x8 unsplit, 32x8 (2 CTAs per SM) split 2
+STAGE_TRAFFIC_FP32 = {(3, 1): 402.10e6, (2, 2): 389.85e6}
 WORKLOAD = "isentropic vortex 3D Euler, periodic [-5,5]^3, 8 uneven blocks, 128^3 = 2,097,152 cells, WENO5 + AUSM, RK4, CFL 0.5"
 
 
@@ -277,10 +280,9 @@ def product(args, dist: Dist):
 
     out["value"] = gcs(ms32)
     out["ms_per_step"] = ms32
-    # DRAM bytes per stage launch (read + write, mean of the 4 launches of one
-    # step) from one ncu capture of the FP32 16x8 kernel on this workload;
-    # null for other workloads
-    traffic = STAGE_TRAFFIC_FP32 if ("fp32" in forms and args.n == 128) else None
+    # DRAM bytes per stage launch from the ncu capture of the tiling the
+    # autotuner chose; null for a tiling or workload not captured
+    traffic = STAGE_TRAFFIC_FP32.get((tz32[0], tz32[2])) if ("fp32" in forms and args.n == 128) else None
     out["roofline"] = roof(prof32, traffic)
     out["clocks"] = clocks
     out["gpu_launches"] = launches * args.steps
