@@ -92,7 +92,7 @@ def save_cache(c: dict) -> None:
         json.dump(c, f, indent=1, sort_keys=True)
 
 
-def autotune(solver, ncells: int, zchunks=(0, 8, 16, 32, 64), tiles=(0, 1, 2, 3), splits=(1, 2), reps: int = 3,
+def autotune(solver, ncells: int, zchunks=(0, 8, 16, 32, 64), tiles=(0, 1, 2, 3), splits=(1, 2, 3, 4), reps: int = 3,
              use_cache=True):
     """Pick (tile, zchunk, tail split) for case 0 of `solver` (state already
     uploaded). Returns (tile, zchunk, ms_per_step, split). Stepping during the
