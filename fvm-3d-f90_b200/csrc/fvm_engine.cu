@@ -706,42 +706,62 @@ int Engine::plan() {
     Group& G = groups[g];
     G.task_off = (int)tasks.size();
     std::vector<Task> gt;
+    // z chunk of the group's cases without a tuned one: the length with the
+    // lowest estimated queue makespan over all the group's tasks. A task of c
+    // planes costs c plane-times plus the warm-up of its z window (WENO: 2
+    // planes of z-only work, MUSCL 1) and its set-up; the queue of T tasks of
+    // total cost S and longest cost M on the kernel's resident CTAs takes M
+    // while T fits on them, else about S / CTAs + (M / 2) (CTAs / T): taken
+    // longest first, the queue ends on short tasks, the more so the more
+    // tasks each CTA takes (on the 64-case batch the estimate picks the
+    // longest chunks, as measured best). Alone, a small case takes short
+    // chunks to spread over the CTAs; in a large batch the warm-ups dominate
+    // and the chunks grow. The estimate costs O(blocks) per candidate, so
+    // the re-plans of a serving loop stay cheap. The state does not depend
+    // on the tiling (only the residual norms' summation order does).
+    int64_t L_auto = 0;
+    if (G.dim == 3) {
+      auto in_group = [&](int ci) { return cases[ci].group == (int)g; };
+      const double ovh = G.recon == FVM_RECON_WENO ? 1.0 : (G.recon == FVM_RECON_MUSCL ? 0.65 : 0.35);
+      struct QStat {
+        double tasks = 0, sum = 0, mx = 0;
+      };
+      auto add_case = [&](const HCase& hc, int64_t L, QStat& q) {
+        for (int bi : hc.blocks) {
+          const HBlock& b = blocks[bi];
+          const int64_t ncol = ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty);
+          const int64_t nc = std::max<int64_t>(1, (b.n[2] + L - 1) / L);  // equal_chunks
+          const int64_t longest = b.n[2] / nc + (b.n[2] % nc ? 1 : 0);
+          q.tasks += (double)(ncol * nc);
+          q.sum += (double)ncol * ((double)b.n[2] + (double)nc * ovh);
+          q.mx = std::max(q.mx, (double)longest + ovh);
+        }
+      };
+      bool any_auto = false;
+      QStat fixed;
+      for (int ci : live_cases) {
+        if (!in_group(ci)) continue;
+        if (cases[ci].zchunk > 0)
+          add_case(cases[ci], cases[ci].zchunk, fixed);
+        else
+          any_auto = true;
+      }
+      double best = 0.0;
+      for (int64_t cand = 64; any_auto && cand >= 4; cand -= (cand > 16 ? 4 : 2)) {
+        QStat q = fixed;
+        for (int ci : live_cases)
+          if (in_group(ci) && cases[ci].zchunk <= 0) add_case(cases[ci], cand, q);
+        const double m = q.tasks <= G.grid ? q.mx : q.sum / G.grid + 0.5 * q.mx * G.grid / q.tasks;
+        if (L_auto <= 0 || m < best * 0.995) {
+          best = m;
+          L_auto = cand;
+        }
+      }
+    }
     for (int ci : live_cases) {
       HCase& hc = cases[ci];
       if (hc.group != (int)g) continue;
-      // z chunk from the case's own size only, so a case is tiled the same
-      // whether it runs alone or batched with others
-      int64_t L = hc.zchunk;
-      if (G.dim == 3 && L <= 0) {
-        if (hc.auto_key == std::make_pair(G.tile, G.grid)) {
-          L = hc.auto_zchunk;
-        } else {
-          // Pick the chunk length whose simulated queue makespan is lowest.
-          // A task of c planes costs c plane-times plus the warm-up of its z
-          // window (WENO: 2 planes of z-only work, MUSCL 1) and its set-up.
-          const double ovh = G.recon == FVM_RECON_WENO ? 1.0 : (G.recon == FVM_RECON_MUSCL ? 0.65 : 0.35);
-          double best = 0.0;
-          std::vector<double> cost;
-          std::vector<int64_t> z0s;
-          for (int64_t cand = 64; cand >= 4; cand -= (cand > 16 ? 4 : 2)) {
-            cost.clear();
-            for (int bi : hc.blocks) {
-              const HBlock& b = blocks[bi];
-              const int64_t ncol = ((b.n[0] + G.k.tx - 1) / G.k.tx) * ((b.n[1] + G.k.ty - 1) / G.k.ty);
-              equal_chunks(b.n[2], cand, z0s);
-              for (size_t c = 0; c + 1 < z0s.size(); ++c)
-                for (int64_t q = 0; q < ncol; ++q) cost.push_back((double)(z0s[c + 1] - z0s[c]) + ovh);
-            }
-            const double m = queue_makespan(cost, G.grid);
-            if (L <= 0 || m < best * 0.995) {
-              best = m;
-              L = cand;
-            }
-          }
-          hc.auto_key = std::make_pair(G.tile, G.grid);
-          hc.auto_zchunk = L;
-        }
-      }
+      const int64_t L = hc.zchunk > 0 ? (int64_t)hc.zchunk : L_auto;
       std::vector<int64_t> z0s;
       std::vector<Task> ct;
       for (int bi : hc.blocks) {

@@ -58,11 +58,8 @@ struct HCase {
   bool dt_stale = true; // state uploaded since the last step: dt is recomputed from it
   int group = -1;
   int tile = -1;        // forced tile (autotuner result), -1 = heuristic
-  int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model
+  int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model over the case's group
   int tail_split = 1;   // pieces each task of the last, partial queue round is cut into (1 = none)
-  // cost-model choice cached per (tile, grid); depends on the case alone
-  std::pair<int, int> auto_key{-1, -1};
-  int64_t auto_zchunk = 0;
 };
 
 struct Group {
