@@ -337,6 +337,42 @@ def product(args, dist: Dist):
                       "ms_per_step": sec * 1e3,
                       "path": "fvm_set_states (8 blocks, pinned) + fvm_step(1) + fvm_get_states per step"}
         s.close()
+        # the same loop on two contexts from two host threads, each advancing
+        # its own state (one context per host thread, as the ABI allows): one
+        # context's upload overlaps the other's download and steps
+        import threading
+
+        pins2 = []
+        for q in case.states:
+            t = torch.empty(q.size, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = q.reshape(-1)
+            pins2.append(t)
+        ctxs = [(fresh(abi.PREC_FP32_FLUX, *tz32), ptrs), (fresh(abi.PREC_FP32_FLUX, *tz32),
+                                                          [t.data_ptr() for t in pins2])]
+        for c, p in ctxs:
+            c.set_states_ptr(blks, p)
+            c.step(1)
+            c.get_states_ptr(blks, p)
+
+        def loop(c, p):
+            for _ in range(ke):
+                c.set_states_ptr(blks, p)
+                c.step(1)
+                c.get_states_ptr(blks, p)
+
+        ths = [threading.Thread(target=loop, args=cp) for cp in ctxs]
+        dist.barrier()
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        sec2 = dist.max((time.perf_counter() - t0) / ke)
+        out["e2e"]["two_contexts"] = {"value": 2 * ncells * stages * dist.world / sec2 / 1e9, "unit": UNIT,
+                                      "ms_per_step_each": sec2 * 1e3,
+                                      "path": "two contexts on two host threads, each the loop above"}
+        for c, _ in ctxs:
+            c.close()
     s32.close()
     return out
 
