@@ -1021,17 +1021,25 @@ int Engine::plan() {
     cases[ci].fresh = false;
     cases[ci].dt_stale = true;
   }
-  void* old[] = {d_blocks_, d_cases_, d_case_blk_, d_tasks_, d_partials_, d_pairs_, d_counters_, d_casemax_};
-  for (void* p : old)
-    if (p) cudaFree(p);
+  // cell offsets within a role slab stay below 2^31 (a slab of 2^31 cells
+  // would take 344 GB in the 4 roles, twice the HBM): 8 bytes per pair.
+  // Checked before the old descriptors are released.
+  if (cap_ >= ((int64_t)1 << 31)) return fail(FVM_ERR_INVALID, "arena too large for 32-bit ghost offsets");
+  // Every pointer is cleared as it is freed, so an allocation failure below
+  // (CK returns early) leaves null members, never freed addresses that the
+  // next plan() or the destructor would free a second time.
+  void** old[] = {(void**)&d_blocks_, (void**)&d_cases_,    (void**)&d_case_blk_, (void**)&d_tasks_,
+                  (void**)&d_partials_, (void**)&d_pairs_, (void**)&d_counters_, (void**)&d_casemax_};
+  for (void** p : old) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+  }
+  planned_ = false;
   CK(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks.size()));
   CK(cudaMalloc(&d_cases_, sizeof(DevCase) * cases.size()));
   CK(cudaMalloc(&d_case_blk_, sizeof(int) * std::max<size_t>(1, case_blk.size())));
   CK(cudaMalloc(&d_tasks_, sizeof(Task) * std::max<size_t>(1, tasks.size())));
   CK(cudaMalloc(&d_partials_, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size())));
-  // cell offsets within a role slab stay below 2^31 (a slab of 2^31 cells
-  // would take 344 GB in the 4 roles, twice the HBM): 8 bytes per pair
-  if (cap_ >= ((int64_t)1 << 31)) return fail(FVM_ERR_INVALID, "arena too large for 32-bit ghost offsets");
   std::vector<int32_t> pairs32(pairs.begin(), pairs.end());
   CK(cudaMalloc(&d_pairs_, sizeof(int32_t) * std::max<size_t>(2, pairs32.size())));
   ncounters_ = max_stages_ * (int)groups.size();
@@ -1510,7 +1518,9 @@ struct fvm_ctx {
   int case_id = 0;
 };
 
-static std::string g_create_error;
+// Per host thread, like the contexts: one thread's failed fvm_create never
+// overwrites the message another thread is reading.
+static thread_local std::string g_create_error;
 
 // Message for fvm_last_error(NULL, ...) from entry points without a context.
 void fvm_internal_set_global_error(const char* msg) { g_create_error = msg ? msg : ""; }
@@ -1641,10 +1651,18 @@ int fvm_run(fvm_ctx* ctx, int64_t max_step, double total_time, double absolute_r
   int why = FVM_STOP_NONE;
   fvm::DevCaseState s;
   std::memset(&s, 0, sizeof s);
+  // a context that has stepped before starts from its current state, so the
+  // stop rules see its step count, time and residuals before any new step
+  if (ctx->eng.has_case_state(ctx->case_id)) {
+    int rc = ctx->eng.read_case_state(ctx->case_id, &s);
+    if (rc) return rc;
+  }
   for (;;) {
-    // converged() (class_iteration.f90, file-local 145-192)
+    // converged() (class_iteration.f90, file-local 145-192); max_step counts
+    // the context's steps from its first one, like the reference's iteration
+    // counter, and a limit already reached stops before any step
     if (s.step != 0) {
-      if (s.step == max_step) why = FVM_STOP_MAX_STEP;
+      if (s.step >= max_step) why = FVM_STOP_MAX_STEP;
       else if (s.t > total_time - time_tol) why = FVM_STOP_MAX_TIME;
       else if (s.res_abs[5] < absolute_residual) why = FVM_STOP_ABS_RESIDUAL;
       else if (s.res_rel[5] < relative_residual) why = FVM_STOP_REL_RESIDUAL;

@@ -93,6 +93,10 @@ class Engine {
   int get_rhs(int blk, double* rhs);
   int step(int nsteps);
   int read_case_state(int case_id, DevCaseState* out);
+  // true once the case's device state exists (read_case_state would succeed)
+  bool has_case_state(int case_id) const {
+    return live_case(case_id) && d_state_ && case_id < state_cap_ && !cases[case_id].fresh;
+  }
 
   // Test hook of the tensor-copy timeout path (see fvm_test_drop_tensor_copies).
   int set_drop_copies(bool on);

@@ -11,8 +11,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <mutex>
-
 #include "../../include/fvm3d.h"
 
 namespace fvm {
@@ -70,16 +68,35 @@ int residual_launch(const double* rhs, const int64_t nvert[3], double* res, doub
 
 }  // namespace fvm
 
+void fvm_internal_set_global_error(const char* msg);
+
 extern "C" int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3], double* res_dev, void* stream) {
-  if (!rhs_dev || !nvert || !res_dev) return FVM_ERR_INVALID;
+  if (!rhs_dev || !nvert || !res_dev) {
+    fvm_internal_set_global_error("fvm_residual_norms: null argument");
+    return FVM_ERR_INVALID;
+  }
   for (int d = 0; d < 3; ++d)
-    if (nvert[d] < 1) return FVM_ERR_INVALID;
-  if (nvert[2] > 0x7fffffff) return FVM_ERR_INVALID;
+    if (nvert[d] < 1) {
+      fvm_internal_set_global_error("fvm_residual_norms: nvert must be >= 1");
+      return FVM_ERR_INVALID;
+    }
+  if (nvert[2] > 0x7fffffff) {
+    fvm_internal_set_global_error("fvm_residual_norms: nvert[2] above 2^31-1 planes");
+    return FVM_ERR_INVALID;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* scratch = nullptr;
-  if (cudaMalloc(&scratch, sizeof(double) * 5 * nvert[2]) != cudaSuccess) return FVM_ERR_NOMEM;
+  if (cudaMalloc(&scratch, sizeof(double) * 5 * nvert[2]) != cudaSuccess) {
+    (void)cudaGetLastError();
+    fvm_internal_set_global_error("fvm_residual_norms: cudaMalloc of the per-plane scratch failed");
+    return FVM_ERR_NOMEM;
+  }
   int rc = fvm::residual_launch(rhs_dev, nvert, res_dev, scratch, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) rc = FVM_ERR_CUDA;
+  if (rc) fvm_internal_set_global_error("fvm_residual_norms: kernel launch failed");
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    rc = FVM_ERR_CUDA;
+    fvm_internal_set_global_error("fvm_residual_norms: the stream reported an error");
+  }
   cudaFree(scratch);
   return rc;
 }
@@ -96,16 +113,10 @@ extern "C" int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3],
 namespace {
 
 constexpr int64_t kNoAllocMaxPlanes = 4096;
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_plane_sums[kNoAllocMaxPlanes * 5];
 
-std::mutex g_noalloc_mu;
-double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
 }  // namespace
-
-void fvm_internal_set_global_error(const char* msg);
 
 extern "C" int fvm_residual_norms_noalloc(const double* rhs_dev, const int64_t nvert[3], double* res_dev,
                                           void* stream) {
@@ -124,30 +135,26 @@ extern "C" int fvm_residual_norms_noalloc(const double* rhs_dev, const int64_t n
         "use fvm_residual_norms");
     return FVM_ERR_INVALID;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return FVM_ERR_CUDA;
-  if (dev < 0 || dev >= kNoAllocMaxDevices) {
-    fvm_internal_set_global_error("fvm_residual_norms_noalloc: device ordinal above 63");
-    return FVM_ERR_UNSUPPORTED;
+  // The array's device address on the current device. Its name in host code
+  // is only a host-side stand-in, so the address is looked up here, with the
+  // caller's device current, on every call: a host-side query that allocates
+  // nothing and so never goes stale (after a cudaDeviceReset the module is
+  // loaded again at a new address). The first call on a device loads the
+  // library's device code there, which is why it belongs before any capture.
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_plane_sums);
+  if (e != cudaSuccess || !p) {
+    (void)cudaGetLastError();
+    fvm_internal_set_global_error("fvm_residual_norms_noalloc: cudaGetSymbolAddress failed on the current device");
+    return FVM_ERR_CUDA;
   }
-  double* scratch = nullptr;
-  {
-    // once per device, with that device current: the array's device address
-    // (its name in host code is only a host-side stand-in)
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_plane_sums);
-      if (e != cudaSuccess || !p) {
-        fvm_internal_set_global_error("fvm_residual_norms_noalloc: cudaGetSymbolAddress failed");
-        return FVM_ERR_CUDA;
-      }
-      g_noalloc_ptr[dev] = static_cast<double*>(p);
-    }
-    scratch = g_noalloc_ptr[dev];
-  }
+  double* scratch = static_cast<double*>(p);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = fvm::residual_launch(rhs_dev, nvert, res_dev, scratch, s);
-  if (cudaStreamSynchronize(s) != cudaSuccess) rc = FVM_ERR_CUDA;
+  if (rc) fvm_internal_set_global_error("fvm_residual_norms_noalloc: kernel launch failed");
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    rc = FVM_ERR_CUDA;
+    fvm_internal_set_global_error("fvm_residual_norms_noalloc: the stream reported an error");
+  }
   return rc;
 }

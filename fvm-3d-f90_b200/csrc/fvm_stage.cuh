@@ -174,6 +174,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
   }
   return false;
 }
+// Error path: wait up to 200 ms for the last armed phase of b (parity
+// `parity`) to complete, so no copy is left writing into shared memory.
+// Returns at once when that phase has already completed (or was never armed
+// since the previous completed wait).
+__device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
+  const uint64_t t0 = global_ns();
+  for (int i = 0; i < (1 << 24); ++i) {
+    if (mbar_try_wait(b, parity)) return;
+    if (global_ns() - t0 > 200000000ull) return;
+  }
+}
 // 4D tiled tensor copy global -> this CTA's shared memory, completing on b.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                             uint64_t* b) {
@@ -855,19 +866,17 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       __syncthreads();
 
       // ---- phase C: rhs, RK update, reductions -------------------------------
+      // fail: a tensor copy of this plane did not arrive in time (seen by this
+      // thread); the CTA decides together at the end of the plane
+      bool fail = false;
       if constexpr (C::TMA) {
-        // every thread waits for the operand boxes issued at the top of this
-        // plane (they leave together if a box does not arrive)
+        // every thread waits for the operand boxes issued at the top of this plane
         if (do_xy) {
-          const bool okq = mbar_wait(&s_mbar[2], ph_q);
+          fail = !mbar_wait(&s_mbar[2], ph_q);
           ph_q ^= 1;
-          if (!okq) {
-            if (tid == 0) atomicExch(a.err, 1);
-            return;
-          }
         }
       }
-      if (do_xy && act) {
+      if (do_xy && act && !fail) {
         constexpr int NF = C::NXF + C::NYF;
         const int fxl = ty * (TX + 1) + tx;
         const int fyl = C::NXF + ty * TX + tx;
@@ -967,20 +976,13 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       if constexpr (C::PSM && !C::TMA) __pipeline_wait_prior(0);
       if constexpr (C::TMA) {
         // every thread waits for the boxes issued at the top of this plane
-        bool ok = true;
         if (more) {
-          ok = mbar_wait(&s_mbar[1], ph_z);
+          fail |= !mbar_wait(&s_mbar[1], ph_z);
           ph_z ^= 1;
         }
-        if (more_xy && ok) {
-          ok = mbar_wait(&s_mbar[0], ph_p);
+        if (more_xy) {
+          fail |= !mbar_wait(&s_mbar[0], ph_p);
           ph_p ^= 1;
-        }
-        if (!ok) {
-          // a copy did not arrive: report it and leave (every thread of the
-          // CTA polls the same barrier, so they leave together)
-          if (tid == 0) atomicExch(a.err, 1);
-          return;
         }
       }
       if (DIM == 3 && colt) {
@@ -1030,7 +1032,24 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
           }
         }
       }
-      __syncthreads();
+      if constexpr (C::TMA) {
+        // The plane's closing barrier also gathers the threads' wait results,
+        // so the whole CTA leaves together even when a copy lands so close to
+        // the deadline that only some threads saw it. Before leaving, thread 0
+        // (the issuer) waits, again bounded, for any copy still in flight, so
+        // none writes into the shared memory of an exited CTA.
+        if (__syncthreads_or(fail)) {
+          if (tid == 0) {
+            atomicExch(a.err, 1);
+            mbar_drain(&s_mbar[0], ph_p ^ 1u);
+            mbar_drain(&s_mbar[1], ph_z ^ 1u);
+            mbar_drain(&s_mbar[2], ph_q ^ 1u);
+          }
+          return;
+        }
+      } else {
+        __syncthreads();
+      }
     }
 
     if (a.last) cta_reduce_store<NT>(sS, s_red, a.partials + (int64_t)T.slot * kPartStride);

@@ -193,7 +193,11 @@ enum fvm_stop {
 /* Run steps until a stop rule of ClassIteration%converged fires: step ==
  * max_step, t > total_time - 1e-10, R_total < absolute_residual, relative
  * R_total < relative_residual. Errors as fvm_step. *steps_done and *reason
- * may be NULL. */
+ * may be NULL. max_step counts the context's steps from its first one (the
+ * reference's iteration counter), not the steps of this call: a second
+ * fvm_run continues from the current step, time and residuals, and returns
+ * at once with FVM_STOP_MAX_STEP (0 steps done) when the count has already
+ * reached max_step. */
 int fvm_run(fvm_ctx* ctx, int64_t max_step, double total_time, double absolute_residual,
             double relative_residual, int64_t* steps_done, int* reason);
 
@@ -233,7 +237,8 @@ int fvm_case_state(fvm_ctx* ctx, int case_id, double* t, double* dt, int64_t* st
 
 /* Autotuner hooks; no counterpart in the reference. fvm_tune_set forces the
  * tile shape (index 0: 32x8, 1: 16x16, 2: 32x8 with registers capped for two
- * resident CTAs per SM; -1 = heuristic) and z chunk length
+ * resident CTAs per SM, 3: 16x8 on 128 threads, the heuristic's choice for 3D
+ * FP32-flux and FP64 cases; -1 = heuristic) and z chunk length
  * (0 = heuristic) of the fused stage kernel for case `case_id`, keeping the
  * current state; fvm_tune_time_step runs `reps` full time steps (the state
  * advances) and returns the mean device time per step in ms.
@@ -271,7 +276,7 @@ int fvm_test_fast_math(const double* x, int64_t n, double* rcp_out, double* rsqr
  * accumulate like the reference (zero them before the first block). Runs on
  * `stream` (a cudaStream_t, NULL for the default stream) and returns after
  * it completes; allocates a scratch buffer of 40 bytes per k plane for the
- * call. */
+ * call. Failures leave a message for fvm_last_error(NULL, ...). */
 int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3], double* res_dev, void* stream);
 
 /* fvm_residual_norms for callers that cannot allocate device memory; no
@@ -281,9 +286,11 @@ int fvm_residual_norms(const double* rhs_dev, const int64_t nvert[3], double* re
  * per-plane scratch from a fixed array inside the library (160 KiB per GPU
  * that loads it, kept until the process exits) and calls no allocator.
  * Limit: nvert[2] <= 4096 planes; larger blocks are rejected with
- * FVM_ERR_INVALID and a message for fvm_last_error(NULL, ...). The first
- * call on a device looks up the array's device address (with that device
- * current); make that first call before any stream capture. All calls share
+ * FVM_ERR_INVALID and a message for fvm_last_error(NULL, ...). Every call
+ * looks up the array's device address on the current device (a host-side
+ * query that allocates nothing); the first call on a device also loads the
+ * library's device code there, so make that first call before any stream
+ * capture. All calls share
  * the array: calls that overlap on the GPU (other host threads, other
  * streams) race, while calls in sequence are safe because every partial the
  * finalize reads is written by the same call first. Returns after `stream`
