@@ -307,6 +307,25 @@ def kinetic_energy(q, dV=1.0):
     return float(0.5 * np.sum((q[1] ** 2 + q[2] ** 2 + q[3] ** 2) / q[0]) * dV)
 
 
+def enstrophy(q, dx, dV=None):
+    """Volume-integrated enstrophy sum 0.5*rho|curl u|^2 dV of a periodic
+    single-block state (5, nk, nj, ni) with uniform spacing dx: the vorticity
+    from second-order central differences, wrapped across every face (the
+    Taylor-Green box). Fixed operation order, so equal states give equal
+    values bit for bit."""
+    dV = dx ** 3 if dV is None else dV
+    rho = q[0]
+    u, v, w = q[1] / rho, q[2] / rho, q[3] / rho
+
+    def d(f, axis):  # axis 2 = x (i), 1 = y (j), 0 = z (k)
+        return (np.roll(f, -1, axis=axis) - np.roll(f, 1, axis=axis)) / (2.0 * dx)
+
+    wx = d(w, 1) - d(v, 0)
+    wy = d(u, 0) - d(w, 2)
+    wz = d(v, 2) - d(u, 1)
+    return float(0.5 * np.sum(rho * (wx * wx + wy * wy + wz * wz)) * dV)
+
+
 # ---------------------------------------------------------------- batched families
 def blast(n=(64, 64, 64), seed=0, **cfg) -> Case:
     """Spherical blast in a unit box: (rho,p) inside / outside a sphere of

@@ -142,3 +142,22 @@ def test_multi_block_state_calls_match_per_block():
     b.set_states({})
     a.close()
     b.close()
+
+
+def test_run_continues_from_the_current_step():
+    # fvm_run's max_step counts the context's steps from its first one (the
+    # reference's iteration counter): a second call continues, and a limit
+    # already reached returns at once with no step
+    c = cases.riemann2d(n=24, seed=1, dt=1e-3)
+    g = c.apply(Solver(c.config()))
+    o = c.apply(orc.Oracle(c.config()))
+    assert g.run(max_step=3) == (3, abi.STOP_MAX_STEP)
+    assert g.run(max_step=5) == (2, abi.STOP_MAX_STEP)
+    assert g.run(max_step=4) == (0, abi.STOP_MAX_STEP)
+    assert g.time()[2] == 5
+    # a time limit already passed stops before any step as well
+    assert g.run(total_time=1e-3) == (0, abi.STOP_MAX_TIME)
+    n, why = g.run(total_time=7e-3)
+    assert why == abi.STOP_MAX_TIME and g.time()[2] == 5 + n
+    o.step(5 + n)
+    assert np.array_equal(g.get_state(0), o.get_state(0))

@@ -64,3 +64,33 @@ def test_permuted_connections_exact(reverse, recon, flux):
     o.step(4)
     for b in range(2):
         assert np.array_equal(g.get_state(b), o.get_state(b)), f"block {b}"
+
+
+@pytest.mark.parametrize("p,periodic,builder", [
+    (6, (True, True, True), "vortex"),
+    (4, (False, False, False), "blast"),
+])
+def test_partitioned_case_gpu_equals_single_block_and_oracle(p, periodic, builder):
+    # partition.partition_case (the IF split of method_partition.f90:576-666)
+    # run on the GPU: the p connected pieces reassemble to the unsplit GPU
+    # run and to the oracle's unsplit run bit for bit
+    from fvm3d import partition
+
+    if builder == "vortex":
+        c1 = cases.isentropic_vortex(N=24, layout="single", rk_stages=3, reconstruct=abi.RECON_MUSCL,
+                                     limiter=abi.LIMITER_MINMOD, flux_split=abi.FLUX_ROE)
+    else:
+        c1 = cases.blast((24, 20, 16), seed=2, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM,
+                         compat=abi.COMPAT_TEXTBOOK)
+    cp = partition.partition_case(c1, p, periodic=periodic)
+    assert len(cp.blocks) == p
+    g1 = c1.apply(Solver(c1.config()))
+    gp = cp.apply(Solver(cp.config()))
+    o1 = c1.apply(orc.Oracle(c1.config()))
+    t1, _, _ = g1.step(3)
+    tp, _, _ = gp.step(3)
+    o1.step(3)
+    qp = cases.assemble(cp, [gp.get_state(b) for b in range(p)])
+    assert np.array_equal(qp, g1.get_state(0))
+    assert np.array_equal(qp, o1.get_state(0))
+    assert t1 == tp
