@@ -9,10 +9,12 @@ AUSM, classic RK4, CFL 0.5. Inputs are the seeded analytic initial state
 (no dataset exists for this solver).
 
 One "step" is one RK4 time step (4 stages) over all blocks. value = cells x
-stages x ranks / max-over-ranks device time, in Gcell-stage/s. The headline
-form computes reconstruction and flux in FP32 with FP64 state and RK
-accumulation; the FP64 plain forms are reported beside it, with the L1
-density difference of the FP32 form against FP64 after the same steps.
+stages x ranks / max-over-ranks device time, in Gcell-stage/s, for the FP64
+plain form (the reference's arithmetic width); the FP32-flux form (FP32
+reconstruction and flux, FP64 state and RK accumulation) and the exact FP64
+form (the reference's operation order) are reported beside it, with the L1
+density difference of the FP32 form against FP64 after the same steps and
+the FP32 / FP64 speed ratio on every configuration.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
@@ -35,10 +37,10 @@ sys.path.insert(0, PKG)
 
 METRIC = "Gcell-stage/s FP64 plain vs FP32-batched at L1 err<=1e-6; served p50/p99 latency"
 UNIT = "Gcell-stage/s"
-# DRAM bytes per stage launch of the FP32 form on the 128^3 vortex (ncu
-# dram__bytes_read.sum + dram__bytes_write.sum, mean of the 4 launches of one
-# step), by (tile index, tail split): 16x8 unsplit, 32x8 (2 CTAs per SM) split 2
-STAGE_TRAFFIC_FP32 = {(3, 1): 402.10e6, (2, 2): 389.85e6}
+# DRAM bytes per stage launch on the 128^3 vortex (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum, mean of the 4 launches of one step), by (precision
+# form, tile index, tail split); tilings not captured report null
+STAGE_TRAFFIC = {}
 WORKLOAD = "isentropic vortex 3D Euler, periodic [-5,5]^3, 8 uneven blocks, 128^3 = 2,097,152 cells, WENO5 + AUSM, RK4, CFL 0.5"
 
 
@@ -55,12 +57,14 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--batch-cases", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-full", action="store_true",
+                    help="serving leg at the full sizes: edges 32..192, 200..2000 steps")
     ap.add_argument("--tile", type=int, default=None, help="fixed tile index (skips the autotuner)")
     ap.add_argument("--zchunk", type=int, default=0, help="fixed z chunk with --tile")
     ap.add_argument("--tail-split", type=int, default=1, help="fixed tail split with --tile (1 = none)")
-    ap.add_argument("--forms", default="fp32,fp64,exact",
-                    help="comma list of arms: fp32 (headline), fp64, exact")
-    ap.add_argument("--only", choices=["tgv", "riemann2d", "accuracy"], default=None,
+    ap.add_argument("--forms", default="fp64,fp32,exact",
+                    help="comma list of precision forms, the first is the headline: fp64, fp32, exact")
+    ap.add_argument("--only", choices=["tgv", "riemann2d", "accuracy", "batched", "serve"], default=None,
                     help="run one secondary leg alone (its precision forms from --forms) and print its JSON")
     ap.add_argument("--accuracy-steps", type=int, default=1000, help="RK4 steps of the accuracy leg")
     return ap.parse_args()
@@ -195,6 +199,25 @@ def peaks() -> dict:
 
 
 # ---------------------------------------------------------------- product arm
+def sig(x, n=4):
+    """x rounded to n significant digits (keeps the JSON line short)."""
+    if x is None or not isinstance(x, float) or x == 0.0 or not math.isfinite(x):
+        return x
+    return round(x, n - 1 - int(math.floor(math.log10(abs(x)))))
+
+
+def timed_windows(solver, k, min_s=1.0, max_windows=64):
+    """Device time per step of k graph-launched steps (CUDA events on the
+    engine's stream, synchronised on both sides), repeated until about
+    min_s seconds of timed work have run. Returns the per-window ms/step."""
+    from fvm3d import tuning
+
+    out = []
+    while len(out) < max_windows and (not out or sum(out) * k < min_s * 1e3):
+        out.append(tuning.time_step(solver, k))
+    return out
+
+
 def product(args, dist: Dist):
     import numpy as np
 
@@ -224,38 +247,18 @@ def product(args, dist: Dist):
         s.close()
         return t, z, sp
 
-    def timed(prec):
+    def timed(prec, clocks=False):
         tile, z, sp = tune(prec)
         s = fresh(prec, tile, z, sp)
         s.step(args.warmup)
         dist.barrier()
-        clk = Clocks(0) if dist.rank == 0 else None
-        ms = tuning.time_step(s, args.steps)
-        clocks = clk.stop() if clk else None
-        ms_max = dist.max(ms)
-        prof = []
-        for _ in range(3):
-            prof.append(tuning.profile_step(s))
+        clk = Clocks(0) if (clocks and dist.rank == 0) else None
+        win = timed_windows(s, args.steps)
+        clk_rec = clk.stop() if clk else None
+        ms = dist.max(statistics.median(win))
+        prof = [tuning.profile_step(s) for _ in range(3)]
         launches = tuning.launches_per_step(s)
-        return s, ms_max, clocks, prof, launches, (tile, z, sp)
-
-    out = {}
-    forms = set(args.forms.split(","))
-    s32 = s64 = sx = None
-    if "fp32" in forms:
-        s32, ms32, clocks, prof32, launches, tz32 = timed(abi.PREC_FP32_FLUX)
-    if "fp64" in forms:
-        s64, ms64, clocks64, prof64, launches64, tz64 = timed(abi.PREC_FP64)
-    if "exact" in forms:
-        sx, msx, clocksx, profx, launchesx, tzx = timed(abi.PREC_FP64_EXACT)
-    if s32 is None:
-        # profiling runs of one FP64 arm only: report it in the headline slots
-        if s64 is not None:
-            s32, ms32, clocks, prof32, launches, tz32 = s64, ms64, clocks64, prof64, launches64, tz64
-            s64 = None
-        else:
-            s32, ms32, clocks, prof32, launches, tz32 = sx, msx, clocksx, profx, launchesx, tzx
-            sx = None
+        return dict(s=s, ms=ms, win=win, clocks=clk_rec, prof=prof, launches=launches, tiling=(tile, z, sp))
 
     def gcs(ms):
         return ncells * stages * dist.world / (ms * 1e-3) / 1e9
@@ -264,170 +267,194 @@ def product(args, dist: Dist):
         return float(np.mean([np.abs(a.get_state(i)[0] - b.get_state(i)[0]).mean() for i in range(nblk)]))
 
     # roofline of the dominant kernel (the fused stage): algorithmic bytes are
-    # the FP64 state arrays each stage must read or write: RK4 stages touch
-    # 3, 5, 5, 4 arrays of 5 x 8 B per cell = 680 B per cell-step.
-    def roof(prof, traffic=None):
+    # the FP64 state arrays each stage must read or write. RK4 with q0 folded
+    # into the accumulator touches 3, 5, 5, 3 arrays of 5 x 8 B per cell:
+    # 640 B per cell-step, 160 B per cell-stage (the same in every precision
+    # form: the state is FP64 in all of them).
+    def roof(r, prec):
+        prof = r["prof"]
         st = [ms for p in prof for k, ms in p if k == "stage"]
         per_step_ms = sum(st) / len(prof)
-        alg = 680.0 * ncells
+        alg = 640.0 * ncells
         ach = alg / (per_step_ms * 1e-3) / 1e9
         pk = peaks()
         share = per_step_ms / (sum(ms for p in prof for _, ms in p) / len(prof))
-        return {"bound": "hbm", "achieved": round(ach, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": round(ach / pk["hbm_gbs"], 4), "traffic": traffic, "peak_src": pk["src"],
-                "stage_ms_per_step": round(per_step_ms, 4), "stage_share_of_step": round(share, 4),
-                "alg_bytes_per_cell_step": 680, "alg_bytes_per_launch": round(170.0 * ncells)}
+        traffic = STAGE_TRAFFIC.get((prec, r["tiling"][0], r["tiling"][2])) if args.n == 128 else None
+        return {"bound": "hbm", "achieved": sig(ach), "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": sig(ach / pk["hbm_gbs"]), "traffic": traffic, "peak_src": pk["src"],
+                "kernel": "stage_kernel", "stage_ms_per_step": sig(per_step_ms), "stage_share_of_step": sig(share),
+                "alg_bytes_per_cell_step": 640, "alg_bytes_per_launch": round(160.0 * ncells)}
 
-    out["value"] = gcs(ms32)
-    out["ms_per_step"] = ms32
-    # DRAM bytes per stage launch from the ncu capture of the tiling the
-    # autotuner chose; null for a tiling or workload not captured
-    traffic = STAGE_TRAFFIC_FP32.get((tz32[0], tz32[2])) if ("fp32" in forms and args.n == 128) else None
-    out["roofline"] = roof(prof32, traffic)
-    out["clocks"] = clocks
-    out["gpu_launches"] = launches * args.steps
-    if s64 is not None:
-        out["fp64_plain"] = {"value": gcs(ms64), "ms_per_step": ms64, "roofline": roof(prof64),
-                             "tile_zchunk": tz64[:2], "tail_split": tz64[2]}
-        # L1 density difference of the FP32-flux form against FP64 after the same steps
-        out["l1_density_err_vs_fp64"] = l1rho(s32, s64)
-    if sx is not None:
-        out["fp64_exact"] = {"value": gcs(msx), "ms_per_step": msx, "roofline": roof(profx), "tile_zchunk": tzx[:2],
-                             "tail_split": tzx[2]}
-        if s64 is not None:
-            out["fp64_plain"]["l1_density_vs_fp64_exact"] = l1rho(s64, sx)
-        else:
-            out["l1_density_err_vs_fp64"] = l1rho(s32, sx)
-    out["tile_zchunk"] = tz32[:2]
-    out["tail_split"] = tz32[2]
-    out["profile_ms"] = {k: round(sum(ms for p in prof32 for kk, ms in p if kk == k) / len(prof32), 4)
-                         for k in ("stage", "gather", "finalize")}
-    for x in (sx, s64):
-        if x is not None:
-            x.close()
+    forms = args.forms.split(",")
+    runs = {}
+    for f in forms:
+        prec = {"fp64": abi.PREC_FP64, "fp32": abi.PREC_FP32_FLUX, "exact": abi.PREC_FP64_EXACT}[f]
+        runs[f] = timed(prec, clocks=(f == forms[0]))
+        runs[f]["prec"] = prec
+    head = runs[forms[0]]
+    out = {"value": gcs(head["ms"]), "ms_per_step": head["ms"],
+           "dtype": {"fp64": "f64", "fp32": "f32 recon/flux, f64 state + RK + dt + norms",
+                     "exact": "f64 (reference operation order)"}[forms[0]],
+           "gpu_launches": head["launches"] * args.steps * len(head["win"]),
+           "roofline": roof(head, head["prec"]), "clocks": head["clocks"]}
+    out["timing"] = {"windows": len(head["win"]), "steps_per_window": args.steps,
+                     "ms_per_step_median": sig(statistics.median(head["win"])),
+                     "ms_per_step_min": sig(min(head["win"])), "ms_per_step_max": sig(max(head["win"])),
+                     "tiling": list(head["tiling"]),
+                     "profile_ms": {k: sig(sum(ms for p in head["prof"] for kk, ms in p if kk == k) / 3)
+                                    for k in ("stage", "gather", "finalize")}}
 
     # end to end through the C ABI with host buffers: every step uploads the
     # state from pinned host memory, advances one step (residuals come back)
-    # and downloads the state.
+    # and downloads the state, in the headline's precision form
     if not args.no_e2e:
-        import torch
+        out["e2e"] = e2e_loop(args, dist, case, fresh, head["prec"], head["tiling"], stages)
 
-        pins = []
+    for f in forms[1:]:
+        r = runs[f]
+        rec = {"value": sig(gcs(r["ms"])), "ms_per_step": sig(r["ms"]), "tiling": list(r["tiling"]),
+               "spread_ms": [sig(min(r["win"])), sig(max(r["win"]))]}
+        if f == "fp32":
+            rec["roofline"] = {k: v for k, v in roof(r, r["prec"]).items()
+                               if k in ("achieved", "frac", "traffic", "stage_ms_per_step")}
+            ref = "fp64" if "fp64" in runs else ("exact" if "exact" in runs else None)
+            if ref:
+                rec["l1_density_vs_" + ref] = sig(l1rho(r["s"], runs[ref]["s"]))
+        out[{"fp64": "fp64_plain", "fp32": "fp32_flux", "exact": "fp64_exact"}[f]] = rec
+    if "fp64" in runs and "exact" in runs and forms[0] == "fp64":
+        out["fp64_exact"]["l1_density_vs_fp64"] = sig(l1rho(runs["exact"]["s"], runs["fp64"]["s"]))
+    if "fp64" in runs and "fp32" in runs:
+        out["vortex_fp32_over_fp64"] = sig(runs["fp64"]["ms"] / runs["fp32"]["ms"])
+    for r in runs.values():
+        r["s"].close()
+    return out
+
+
+def e2e_loop(args, dist, case, fresh, prec, tiling, stages):
+    """fvm_set_states (all blocks, pinned host memory) + fvm_step(1) +
+    fvm_get_states per step, one context; then the same loop on two contexts
+    from two host threads (one context per host thread, as the ABI allows),
+    one's upload overlapping the other's download."""
+    import threading
+
+    import torch
+
+    ncells = case.ncells
+
+    def pinned():
+        ps = []
         for q in case.states:
             t = torch.empty(q.size, dtype=torch.float64, pin_memory=True)
             t.numpy()[:] = q.reshape(-1)
-            pins.append(t)
-        s = fresh(abi.PREC_FP32_FLUX, *tz32)
-        blks = list(range(len(pins)))
-        ptrs = [t.data_ptr() for t in pins]
-        s.set_states_ptr(blks, ptrs)  # warm-up
+            ps.append(t)
+        return ps
+
+    pins = pinned()
+    s = fresh(prec, *tiling)
+    blks = list(range(len(pins)))
+    ptrs = [t.data_ptr() for t in pins]
+    s.set_states_ptr(blks, ptrs)  # warm-up
+    s.step(1)
+    s.get_states_ptr(blks, ptrs)
+    ke = max(3, min(args.steps, 10))
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        s.set_states_ptr(blks, ptrs)
         s.step(1)
         s.get_states_ptr(blks, ptrs)
-        ke = max(3, min(args.steps, 10))
-        dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(ke):
-            s.set_states_ptr(blks, ptrs)
-            s.step(1)
-            s.get_states_ptr(blks, ptrs)
-        sec = (time.perf_counter() - t0) / ke
-        sec = dist.max(sec)
-        out["e2e"] = {"value": ncells * stages * dist.world / sec / 1e9, "unit": UNIT,
-                      "h2d_bytes_per_step": ncells * 40, "d2h_bytes_per_step": ncells * 40 + 2 * 6 * 8 + 8,
-                      "ms_per_step": sec * 1e3,
-                      "path": "fvm_set_states (8 blocks, pinned) + fvm_step(1) + fvm_get_states per step"}
-        s.close()
-        # the same loop on two contexts from two host threads, each advancing
-        # its own state (one context per host thread, as the ABI allows): one
-        # context's upload overlaps the other's download and steps
-        import threading
+    sec = dist.max((time.perf_counter() - t0) / ke)
+    s.close()
+    rec = {"value": ncells * stages * dist.world / sec / 1e9, "unit": UNIT,
+           "h2d_bytes_per_step": ncells * 40, "d2h_bytes_per_step": ncells * 40 + 2 * 6 * 8 + 8,
+           "ms_per_step": sig(sec * 1e3), "path": "fvm_set_states + fvm_step(1) + fvm_get_states, pinned host"}
+    pins2 = pinned()
+    ctxs = [(fresh(prec, *tiling), ptrs), (fresh(prec, *tiling), [t.data_ptr() for t in pins2])]
+    for c, p in ctxs:
+        c.set_states_ptr(blks, p)
+        c.step(1)
+        c.get_states_ptr(blks, p)
 
-        pins2 = []
-        for q in case.states:
-            t = torch.empty(q.size, dtype=torch.float64, pin_memory=True)
-            t.numpy()[:] = q.reshape(-1)
-            pins2.append(t)
-        ctxs = [(fresh(abi.PREC_FP32_FLUX, *tz32), ptrs), (fresh(abi.PREC_FP32_FLUX, *tz32),
-                                                          [t.data_ptr() for t in pins2])]
-        for c, p in ctxs:
+    def loop(c, p):
+        for _ in range(ke):
             c.set_states_ptr(blks, p)
             c.step(1)
             c.get_states_ptr(blks, p)
 
-        def loop(c, p):
-            for _ in range(ke):
-                c.set_states_ptr(blks, p)
-                c.step(1)
-                c.get_states_ptr(blks, p)
-
-        ths = [threading.Thread(target=loop, args=cp) for cp in ctxs]
-        dist.barrier()
-        t0 = time.perf_counter()
-        for th in ths:
-            th.start()
-        for th in ths:
-            th.join()
-        sec2 = dist.max((time.perf_counter() - t0) / ke)
-        out["e2e"]["two_contexts"] = {"value": 2 * ncells * stages * dist.world / sec2 / 1e9, "unit": UNIT,
-                                      "ms_per_step_each": sec2 * 1e3,
-                                      "path": "two contexts on two host threads, each the loop above"}
-        for c, _ in ctxs:
-            c.close()
-    s32.close()
-    return out
+    ths = [threading.Thread(target=loop, args=cp) for cp in ctxs]
+    dist.barrier()
+    t0 = time.perf_counter()
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    sec2 = dist.max((time.perf_counter() - t0) / ke)
+    rec["two_contexts"] = sig(2 * ncells * stages * dist.world / sec2 / 1e9)
+    for c, _ in ctxs:
+        c.close()
+    return rec
 
 
 # ---------------------------------------------------------------- batched leg
 def batched(args):
     """64 independent 3D Euler cases (seeded blasts / oblique shock tubes,
     grid edges round(32 * 4**u), u ~ U[0,1] per axis, random Roe / AUSM x
-    MUSCL / WENO5, SSP-RK3, FP32 flux, TEXTBOOK compat: the reference's WENO
-    goes to NaN on the strongest blasts) advanced together: one persistent
-    launch per scheme group and stage, one CUDA graph per step. Compared with
-    the same cases run one engine at a time (sum of their device times)."""
+    MUSCL / WENO5, SSP-RK3, TEXTBOOK compat: the reference's WENO goes to NaN
+    on the strongest blasts) advanced together: one persistent launch per
+    scheme group and stage, one CUDA graph per step; in the FP32-flux and the
+    FP64 forms. The FP32 batch is also compared with the same cases run one
+    engine at a time (sum of their device times)."""
     import numpy as np
 
     from fvm3d import abi, cases, tuning
     from fvm3d.solver import Solver
 
-    rng = np.random.default_rng(2024)
-    cs = []
-    for i in range(args.batch_cases):
-        n = tuple(int(round(32 * 4 ** u)) for u in rng.uniform(size=3))
-        recon = [abi.RECON_MUSCL, abi.RECON_WENO][int(rng.integers(2))]
-        flux = [abi.FLUX_ROE, abi.FLUX_AUSM][int(rng.integers(2))]
-        fam = cases.blast if rng.uniform() < 0.5 else cases.shock_tube
-        cs.append(fam(n, seed=int(rng.integers(1 << 30)), reconstruct=recon, flux_split=flux,
-                      limiter=abi.LIMITER_MINMOD, kappa=1.0 / 3.0, precision=abi.PREC_FP32_FLUX,
-                      compat=abi.COMPAT_TEXTBOOK))
-    cells = sum(c.ncells for c in cs)
+    def build(prec):
+        rng = np.random.default_rng(2024)
+        cs = []
+        for i in range(args.batch_cases):
+            n = tuple(int(round(32 * 4 ** u)) for u in rng.uniform(size=3))
+            recon = [abi.RECON_MUSCL, abi.RECON_WENO][int(rng.integers(2))]
+            flux = [abi.FLUX_ROE, abi.FLUX_AUSM][int(rng.integers(2))]
+            fam = cases.blast if rng.uniform() < 0.5 else cases.shock_tube
+            cs.append(fam(n, seed=int(rng.integers(1 << 30)), reconstruct=recon, flux_split=flux,
+                          limiter=abi.LIMITER_MINMOD, kappa=1.0 / 3.0, precision=prec,
+                          compat=abi.COMPAT_TEXTBOOK))
+        return cs
+
     steps = max(3, min(args.steps, 20))
-    s = Solver(cs[0].config())
-    s.remove_case(0)
-    for c in cs:
-        cid = s.add_case(c.config())
-        c.case_id = cid
-        c.apply(s, case_id=cid, states=False)
-    for c in cs:
-        for b, q in enumerate(c.states):
-            s.set_state(c.block_ids[b], q)
-    s.step(2)
-    ms = tuning.time_step(s, steps)
-    failed = sum(1 for c in cs if s.case_state(c.case_id)["status"] != 0)
-    groups = len({(c.cfg["reconstruct"], c.cfg["flux_split"]) for c in cs})
-    launches = tuning.launches_per_step(s)
-    s.close()
-    seq_ms = 0.0
-    for c in cs:
-        a = c.apply(Solver(c.config()))
-        a.step(1)
-        seq_ms += tuning.time_step(a, steps)
-        a.close()
-    return {"cases": len(cs), "cells": cells, "scheme_groups": groups, "steps": steps, "ms_per_step": ms,
-            "cases_nonfinite": failed,
-            "value": cells * 3 / (ms * 1e-3) / 1e9, "unit": UNIT, "kernel_launches_per_step": launches,
-            "one_at_a_time": {"ms_per_step": seq_ms, "value": cells * 3 / (seq_ms * 1e-3) / 1e9},
-            "dtype": "f32 recon/flux, f64 state"}
+    out = {"cases": args.batch_cases, "steps": steps, "unit": UNIT}
+    for name, prec in (("fp64", abi.PREC_FP64), ("fp32_flux", abi.PREC_FP32_FLUX)):
+        cs = build(prec)
+        cells = sum(c.ncells for c in cs)
+        s = Solver(cs[0].config())
+        s.remove_case(0)
+        for c in cs:
+            cid = s.add_case(c.config())
+            c.case_id = cid
+            c.apply(s, case_id=cid, states=False)
+        for c in cs:
+            for b, q in enumerate(c.states):
+                s.set_state(c.block_ids[b], q)
+        s.step(2)
+        win = timed_windows(s, steps, min_s=0.5)
+        ms = statistics.median(win)
+        failed = sum(1 for c in cs if s.case_state(c.case_id)["status"] != 0)
+        out["cells"] = cells
+        out["scheme_groups"] = len({(c.cfg["reconstruct"], c.cfg["flux_split"]) for c in cs})
+        out[name] = {"value": sig(cells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms), "nonfinite": failed,
+                     "launches_per_step": tuning.launches_per_step(s)}
+        s.close()
+        if name == "fp32_flux":
+            seq_ms = 0.0
+            for c in cs:
+                a = c.apply(Solver(c.config()))
+                a.step(1)
+                seq_ms += tuning.time_step(a, steps)
+                a.close()
+            out[name]["one_at_a_time"] = sig(cells * 3 / (seq_ms * 1e-3) / 1e9)
+    out["fp32_over_fp64"] = sig(out["fp64"]["ms_per_step"] / out["fp32_flux"]["ms_per_step"])
+    return out
 
 
 # ---------------------------------------------------------------- Navier-Stokes leg
@@ -458,12 +485,13 @@ def tgv(args):
         ms = tuning.time_step(s, steps)
         prof = tuning.profile_step(s)
         ke[name] = cases.kinetic_energy(s.get_state(0), dV)
-        out[name] = {"ms_per_step": ms, "value": c.ncells * 3 / (ms * 1e-3) / 1e9, "tile_zchunk_split": [t, z, sp],
-                     "profile_ms": {k: round(sum(x for kk, x in prof if kk == k), 4)
+        out[name] = {"value": sig(c.ncells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms), "tiling": [t, z, sp],
+                     "profile_ms": {k: sig(sum(x for kk, x in prof if kk == k))
                                     for k in ("stage", "viscous", "gather", "finalize")}}
         s.close()
     if len(ke) == 2:
-        out["ke_rel_diff_fp32_vs_fp64"] = abs(ke["fp32_flux"] - ke["fp64"]) / ke["fp64"]
+        out["ke_rel_diff_fp32_vs_fp64"] = sig(abs(ke["fp32_flux"] - ke["fp64"]) / ke["fp64"])
+        out["fp32_over_fp64"] = sig(out["fp64"]["ms_per_step"] / out["fp32_flux"]["ms_per_step"])
     out["unit"] = UNIT
     return out
 
@@ -526,41 +554,49 @@ def riemann2d_leg(args):
             continue
         s = c.apply(Solver(c.config(precision=prec)))
         s.step(3)
-        ms = tuning.time_step(s, steps)
-        out[name] = {"ms_per_step": ms, "value": c.ncells * 3 / (ms * 1e-3) / 1e9}
+        ms = statistics.median(timed_windows(s, steps, min_s=0.3))
+        out[name] = {"value": sig(c.ncells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms)}
         s.close()
+    if "fp64" in out and "fp32_flux" in out:
+        out["fp32_over_fp64"] = sig(out["fp64"]["ms_per_step"] / out["fp32_flux"]["ms_per_step"])
     out["unit"] = UNIT
-    out["note"] = "65,536 cells fill a fraction of the GPU: launch- and latency-bound (3 stage launches per step)"
     return out
 
 
 # ---------------------------------------------------------------- serving leg
 def serve(args):
-    """Poisson stream of seeded 3D Euler requests (blast / shock tube, cubes
-    of 32^3..96^3 cells, 100..400 SSP-RK3 steps, random schemes, FP32 flux)
-    served with continuous batching in a 4 GB state budget, against the same
-    stream served one request at a time."""
+    """Poisson stream of seeded requests from the three solver
+    configurations' families (2D four-quadrant Riemann problem, 8-block
+    isentropic vortex with RK4, Navier-Stokes Taylor-Green vortex; grid edge
+    log-uniform in 32..96, 100..400 steps; 32..192 and 200..2000 steps with
+    --serve-full) in the FP32-flux form, served with continuous batching by
+    the library's server, against the same stream served one request at a
+    time in the plain FP64 form."""
     from fvm3d import abi, serving
 
-    make = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(32, 96))
-    budget = int(4e9 / (5 * 8 * 3))
-    rate = 40.0
+    lo, hi, steps = (32, 192, (200, 2000)) if args.serve_full else (32, 96, (100, 400))
+    make = serving.config_families(precision=abi.PREC_FP32_FLUX, sizes=(lo, hi))
+    budget = int((16e9 if args.serve_full else 4e9) / (5 * 8 * 4))
+    rate = 40.0 if not args.serve_full else 4.0
     out = {}
-    st = serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=(100, 400))
-    srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=1 << 20)
-    out["continuous_batching"] = srv.run(st)
+
+    def short(st):
+        return {k: sig(float(st[k])) if isinstance(st[k], float) else st[k]
+                for k in ("requests", "p50_s", "p99_s", "gcell_stage_per_s", "failed")}
+
+    def stream():
+        return serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=steps)
+
+    srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=1 << 21)
+    out["continuous_batching"] = short(srv.run(stream()))
     srv.close()
-    st = serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=(100, 400))
     srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=None)
-    out["continuous_batching_uncapped"] = srv.run(st)
+    out["continuous_batching_uncapped"] = short(srv.run(stream()))
     srv.close()
-    st = serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=(100, 400))
-    out["one_at_a_time"] = serving.serve_one_at_a_time(st)
+    out["one_at_a_time_fp64"] = short(serving.serve_one_at_a_time(stream(), precision=abi.PREC_FP64))
     out["arrival_rate_per_s"] = rate
-    out["admission"] = "FCFS into a 4 GB arena, running set capped at 2^20 cells (uncapped shown beside)"
-    out["budget_bytes"] = budget * 5 * 8 * 3
-    out["workload"] = ("seeded blasts / oblique shock tubes, 32^3..96^3, 100..400 RK3 steps, Poisson arrivals; "
-                       "reduced from 32^3..192^3 / 200..2000 steps to keep the bench within minutes")
+    out["workload"] = (f"Riemann-2D / 8-block vortex (RK4) / NS TGV, edge {lo}..{hi} (2D: edge^1.5), "
+                       f"{steps[0]}..{steps[1]} steps, FP32 flux; budget {budget * 160 / 1e9:.0f} GB")
     return out
 
 
@@ -609,7 +645,8 @@ def main():
         return
 
     if args.only:
-        leg = {"tgv": tgv, "riemann2d": riemann2d_leg, "accuracy": accuracy_leg}[args.only]
+        leg = {"tgv": tgv, "riemann2d": riemann2d_leg, "accuracy": accuracy_leg, "batched": batched,
+               "serve": serve}[args.only]
         if dist.rank == 0:
             print(json.dumps({"leg": args.only, **leg(args)}))
         dist.close()
@@ -617,19 +654,11 @@ def main():
 
     res = product(args, dist)
     line = dict(base)
-    line.update({"value": res.pop("value"), "ms_per_step": res.pop("ms_per_step"),
-                 "dtype": "f32 recon/flux, f64 state + RK + dt + norms"})
-    line.update(res)
-    if dist.world == 1 and not args.no_batch:
-        line["batched"] = batched(args)
-    if dist.world == 1 and not args.no_batch:
-        line["navier_stokes_tgv"] = tgv(args)
-        line["riemann2d_256"] = riemann2d_leg(args)
-    if dist.world == 1 and not args.no_serve:
-        sv = serve(args)
-        line["serving"] = sv
-        line["p50_s"] = sv["continuous_batching"]["p50_s"]
-        line["p99_s"] = sv["continuous_batching"]["p99_s"]
+    line.update({"value": res.pop("value"), "ms_per_step": res.pop("ms_per_step"), "dtype": res.pop("dtype"),
+                 "gpu_launches": res.pop("gpu_launches"), "roofline": res.pop("roofline"),
+                 "clocks": res.pop("clocks")})
+    if "e2e" in res:
+        line["e2e"] = res.pop("e2e")
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         v, th, sec = cpu_oracle(args.n, 30, 1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
@@ -637,8 +666,32 @@ def main():
                                           f"threads ({sec:.1f} s; C++ restatement of the reference path)"}
         # the reference itself is serial: the same restatement on one thread
         v1, _, sec1 = cpu_oracle(args.n, 3, 0, threads=1)
-        line["cpu_baseline_1thread"] = {"value": v1, "unit": UNIT, "cores": 1, "kind": "port",
-                                        "sample": f"3 RK4 steps of the full 8-block case on one thread ({sec1:.1f} s)"}
+        line["cpu_baseline_1thread"] = {"value": sig(v1), "cores": 1, "sample": f"3 RK4 steps ({sec1:.1f} s)"}
+    line["timing"] = res.pop("timing")
+    ratios = {}
+    if "vortex_fp32_over_fp64" in res:
+        ratios["vortex"] = res.pop("vortex_fp32_over_fp64")
+    if dist.world == 1 and not args.no_serve:
+        sv = serve(args)
+        line["serving"] = sv
+        line["p50_s"] = sv["continuous_batching"]["p50_s"]
+        line["p99_s"] = sv["continuous_batching"]["p99_s"]
+    if dist.world == 1 and not args.no_batch:
+        b = batched(args)
+        line["batched"] = b
+        ratios["batch"] = b["fp32_over_fp64"]
+        t = tgv(args)
+        line["navier_stokes_tgv"] = t
+        ratios["tgv"] = t.get("fp32_over_fp64")
+        r2 = riemann2d_leg(args)
+        line["riemann2d_256"] = r2
+        ratios["riemann2d"] = r2.get("fp32_over_fp64")
+    # the precision forms beside the headline, and the FP32 / FP64 speed
+    # ratio of every configuration, last (the end of the line is what a
+    # truncated log keeps)
+    line.update(res)
+    if ratios:
+        line["fp32_over_fp64"] = ratios
     if dist.rank == 0:
         print(json.dumps(line))
     dist.close()

@@ -403,6 +403,9 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
     double* rhs_out = a.last ? B.rhs : nullptr;
     const bool need_um = (rk_stages == 3 && a.m >= 2);
     const bool need_acc = (rk_stages == 4 && a.m >= 2);
+    // RK4 folds q0 into its accumulator, so stage 4 reads no q0 (local time
+    // steps still need it: the cell's dt comes from its q0)
+    const bool need_u0 = !(rk_stages == 4 && a.m == 4) || ts_set == 2;
 
     const int nxt = min(TX, G.n0 - T.x0), nyt = min(TY, G.n1 - T.y0);
     const bool act = colt && tx < nxt && ty < nyt;
@@ -539,17 +542,17 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         // TMA kernels: the operands of the whole tile as [5][TY][TX] boxes of
         // plane k (the layout of sQ), straight into shared memory
         if (do_xy && tid == 0) {
-          const int nb = 1 + ((need_um || need_acc) ? 1 : 0);
+          const int nb = (need_u0 ? 1 : 0) + ((need_um || need_acc) ? 1 : 0);
           mbar_expect_tx(&s_mbar[2], sizeof(double) * 5 * TY * TX * nb);
           const int bx = T.x0 + kPadX, by = T.y0 + kGhost, bz = k + kGhost;
-          tma_load_4d(sQ, tmb + a.rq0 * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
+          if (need_u0) tma_load_4d(sQ, tmb + a.rq0 * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
           if (need_um) tma_load_4d(sQ + 5 * NC, tmb + a.rin * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
           if (need_acc) tma_load_4d(sQ + 5 * NC, tmb + a.racc * 2 + 1, bx, by, bz, 0, &s_mbar[2]);
         }
       } else if (do_xy && act) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          __pipeline_memcpy_async(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs, sizeof(double));
+          if (need_u0) __pipeline_memcpy_async(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs, sizeof(double));
           if (need_um) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NC + tid, qin + off_k + v * vs, sizeof(double));
           if (need_acc) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NC + tid, accp + off_k + v * vs, sizeof(double));
         }
@@ -936,24 +939,28 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
             for (int v = 0; v < 5; ++v) out[v] = 1.0 / 3.0 * u0[v] + 2.0 / 3.0 * um[v] + c3 * rhs[v];
           }
         } else {
+          // classic RK4 with q0 folded into the accumulator:
+          //   acc = q0 + h/6 k1, acc += h/3 k2, acc += h/3 k3, q = acc + h/6 k4
+          // so the last stage reads the accumulator alone (3, 5, 5, 3 state
+          // arrays per stage)
           if (a.m == 1) {
-            const double h2 = 0.5 * h;
+            const double h2 = 0.5 * h, h6 = h / 6.0;
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-              accp[off + v * vs] = rhs[v];
+              accp[off + v * vs] = u0[v] + h6 * rhs[v];
               out[v] = u0[v] + h2 * rhs[v];
             }
           } else if (a.m == 2 || a.m == 3) {
-            const double hc = (a.m == 2) ? 0.5 * h : h;
+            const double hc = (a.m == 2) ? 0.5 * h : h, h3 = h / 3.0;
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
-              accp[off + v * vs] = ac[v] + 2.0 * rhs[v];
+              accp[off + v * vs] = ac[v] + h3 * rhs[v];
               out[v] = u0[v] + hc * rhs[v];
             }
           } else {
             const double h6 = h / 6.0;
 #pragma unroll
-            for (int v = 0; v < 5; ++v) out[v] = u0[v] + h6 * (ac[v] + rhs[v]);
+            for (int v = 0; v < 5; ++v) out[v] = ac[v] + h6 * rhs[v];
           }
         }
 #pragma unroll

@@ -134,6 +134,52 @@ def make_config(**kw) -> FvmConfig:
     return c
 
 
+class ServerConfig(ctypes.Structure):
+    """struct fvm_server_config of include/fvm3d.h."""
+
+    _fields_ = [
+        ("struct_size", ctypes.c_int32),
+        ("chunk_steps", ctypes.c_int32),
+        ("budget_cells", ctypes.c_int64),
+        ("max_active_cells", ctypes.c_int64),
+        ("max_queued", ctypes.c_int32),
+        ("pad_", ctypes.c_int32),
+    ]
+
+
+class Connection(ctypes.Structure):
+    """struct fvm_connection of include/fvm3d.h."""
+
+    _fields_ = [
+        ("blk", ctypes.c_int32),
+        ("donor", ctypes.c_int32),
+        ("range", (ctypes.c_int64 * 2) * 3),
+        ("donor_range", (ctypes.c_int64 * 2) * 3),
+        ("donor_type", ctypes.c_int32 * 3),
+        ("pad_", ctypes.c_int32),
+    ]
+
+
+class Request(ctypes.Structure):
+    """struct fvm_request of include/fvm3d.h."""
+
+    _fields_ = [
+        ("struct_size", ctypes.c_int32),
+        ("nblocks", ctypes.c_int32),
+        ("cfg", ctypes.POINTER(FvmConfig)),
+        ("nvert", ctypes.POINTER(ctypes.c_int64)),
+        ("dr", ctypes.POINTER(ctypes.c_double)),
+        ("q", ctypes.POINTER(ctypes.POINTER(ctypes.c_double))),
+        ("nbc", ctypes.c_int32),
+        ("nconn", ctypes.c_int32),
+        ("bc", ctypes.POINTER(ctypes.c_int32)),
+        ("conn", ctypes.POINTER(Connection)),
+        ("steps", ctypes.c_int64),
+    ]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "csrc", "lib", "libfvm3d.so")
 
@@ -182,6 +228,16 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "fvm_remove_case": (ctypes.c_int, [vp, ctypes.c_int]),
         "fvm_case_state": (ctypes.c_int, [vp, ctypes.c_int, P(dbl), P(dbl), P(i64), P(dbl), P(dbl),
                                           P(ctypes.c_int)]),
+        "fvm_server_config_default": (ctypes.c_int, [P(ServerConfig)]),
+        "fvm_server_create": (ctypes.c_int, [P(ServerConfig), P(vp)]),
+        "fvm_case_submit": (ctypes.c_int, [vp, P(Request), P(i64)]),
+        "fvm_poll": (ctypes.c_int, [vp, i64, P(ctypes.c_int), P(i64), P(dbl), P(dbl), P(ctypes.c_int)]),
+        "fvm_wait": (ctypes.c_int, [vp, i64, dbl, P(ctypes.c_int)]),
+        "fvm_fetch_state": (ctypes.c_int, [vp, i64, ctypes.c_int, P(dbl)]),
+        "fvm_release": (ctypes.c_int, [vp, i64]),
+        "fvm_server_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_size_t]),
+        "fvm_server_destroy": (ctypes.c_int, [vp]),
+        "fvm_server_stats": (ctypes.c_int, [vp, P(i64), P(i64), P(ctypes.c_int), P(ctypes.c_int)]),
     }
     for name, (res, args) in proto.items():
         f = getattr(lib, name)

@@ -1,13 +1,15 @@
-"""Serving loop: continuous batching of solver requests on one GPU.
+"""Serving: continuous batching of solver requests on one GPU.
 
-Requests (a seeded case plus a number of RK steps) arrive over time. The
-server keeps every admitted case's state resident in one engine whose state
-arena is reserved up front (the HBM budget); a request is admitted, first come
-first served, as soon as its blocks fit into the free arena, and it joins the
-running batch at the next step boundary: all admitted cases advance together,
-one persistent launch per stage. A finished case is read back and removed,
-which frees its arena range for the queue. Time-to-solution is measured from
-arrival to the moment its final state is on the host.
+Requests (a seeded case plus a number of RK steps) arrive over time and are
+submitted to the library's server (fvm_server_* of include/fvm3d.h). Its
+worker thread keeps every admitted case's state resident in engines whose
+state arenas are reserved up front (the HBM budget); a request is admitted,
+first come first served, as soon as its blocks fit into the free arena, and it
+joins the running batch at the next step boundary: all admitted cases advance
+together, one persistent launch per scheme group and stage. A finished case
+is read back and removed, which frees its arena range for the queue.
+Time-to-solution is measured from submission (at arrival) to the moment its
+final state is in host memory.
 
 The one-at-a-time baseline serves the same stream in arrival order with one
 engine per request.
@@ -17,6 +19,7 @@ its neighbours, so a case's final state is the same alone and in the mix.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import time
 from dataclasses import dataclass, field
@@ -35,8 +38,10 @@ class Request:
     arrival: float                # seconds after the stream starts
     cells: int = 0                # arena cells the request needs
     case_id: int = -1
+    req_id: int = -1              # the library server's request id
     remaining: int = 0
     admitted: float = math.nan
+    submitted: float = math.nan
     finished: float = math.nan
     result: list = field(default_factory=list)
     status: int = 0
@@ -81,112 +86,180 @@ def mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(32, 96)):
     return make
 
 
-class Server:
-    """Continuous-batching server over one engine with a fixed state arena."""
+def config_families(precision=abi.PREC_FP32_FLUX, sizes=(32, 96)):
+    """Case builder for the served stream of the three solver configurations'
+    families, drawn with equal probability, grid edge N log-uniform in
+    `sizes` (a 2D case takes edge round(N^1.5), the same cell count as N^3):
+      * four-quadrant 2D Riemann problem, MUSCL / minmod + Roe (fix 0.2),
+        SSP-RK3, CFL 0.5, seeded quadrant states;
+      * 3D Euler isentropic vortex in the 8 uneven periodic blocks, WENO5 +
+        AUSM, classic RK4, CFL 0.5;
+      * 3D Navier-Stokes Taylor-Green vortex (Re 1600, Ma 0.1), MUSCL / Van
+        Albada + Roe + central viscous fluxes, SSP-RK3, CFL 0.5."""
+    def make(rng, i):
+        n = int(round(sizes[0] * (sizes[1] / sizes[0]) ** rng.uniform()))
+        n = max(8, n)
+        fam = int(rng.integers(3))
+        if fam == 0:
+            return cases.riemann2d(n=int(round(n ** 1.5)), seed=int(rng.integers(1 << 30)), precision=precision,
+                                   timestep_set=abi.DT_CFL, cfl=0.5)
+        if fam == 1:
+            return cases.isentropic_vortex(N=n, layout="blocks8", precision=precision)
+        return cases.taylor_green(N=n, precision=precision)
+    return make
 
-    def __init__(self, budget_cells: int, rk_stages: int = 3, chunk: int = 8, max_active_cells: int | None = 1 << 20):
-        """budget_cells: the state arena (HBM budget). max_active_cells: stop
-        admitting once the running set holds this many cells (None = no cap;
-        one request is always admitted into an empty set). Past the point
-        where the running set keeps the GPU busy, admitting more only shares
-        it among more requests, which lengthens every running request's
-        latency: on a B200, a cap of 2^20 cells measured p50 0.22 s against
-        0.45 s uncapped on the bench's 40 requests/s stream, at 4 % lower
-        throughput."""
-        # the context's own first case is only a placeholder for the engine
-        self.s = Solver(abi.make_config(rk_stages=rk_stages))
-        self.s.remove_case(0)
-        self.s.reserve(budget_cells)
+
+class Server:
+    """Continuous-batching server of the library (fvm_server_* in
+    include/fvm3d.h): requests are submitted to a worker thread inside
+    libfvm3d.so that admits them first come, first served, into a reserved
+    state arena (the HBM budget), advances all admitted cases together and
+    retires each one when its steps are done. This class only converts cases
+    to requests and reads results back."""
+
+    def __init__(self, budget_cells: int, chunk: int = 8, max_active_cells: int | None = 1 << 20,
+                 max_queued: int = 4096):
+        """budget_cells: the state arena (HBM budget) in fvm_block_cells
+        units. max_active_cells: stop admitting once the running set holds
+        this many cells (None = no cap; one request is always admitted into
+        an empty set). Past the point where the running set keeps the GPU
+        busy, admitting more only shares it among more requests, which
+        lengthens every running request's latency."""
+        self.lib = abi.load_library()
+        cfg = abi.ServerConfig()
+        self.lib.fvm_server_config_default(ctypes.byref(cfg))
+        cfg.chunk_steps = int(chunk)
+        cfg.budget_cells = int(budget_cells)
+        cfg.max_active_cells = 0 if max_active_cells is None else int(max_active_cells)
+        cfg.max_queued = int(max_queued)
+        self.h = ctypes.c_void_p()
+        rc = self.lib.fvm_server_create(ctypes.byref(cfg), ctypes.byref(self.h))
+        if rc:
+            raise FvmError(rc, "fvm_server_create failed")
         self.budget = budget_cells
-        self.free = budget_cells
-        self.chunk = chunk
-        self.max_active_cells = max_active_cells
-        self.active: list[Request] = []
-        self.steps_run = 0
 
     def close(self):
-        self.s.close()
+        if getattr(self, "h", None):
+            self.lib.fvm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc: int):
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.fvm_server_last_error(self.h, buf, 512)
+            raise FvmError(rc, buf.value.decode())
 
     def cells_of(self, c: cases.Case) -> int:
         idim = int(c.cfg.get("idimension", 3))
         return sum(abi.block_cells(idim, n) for n, _ in c.blocks)
 
-    def fits(self, r: Request) -> bool:
-        if r.cells > self.free:
-            return False
-        if self.max_active_cells is not None and self.active:
-            return sum(a.cells for a in self.active) + r.cells <= self.max_active_cells
-        return True
+    def submit(self, case: cases.Case, nsteps: int) -> int:
+        """fvm_case_submit: the library copies everything before it returns."""
+        nb = len(case.blocks)
+        cfg = case.config()
+        nvert = (ctypes.c_int64 * (3 * nb))(*[int(x) for n, _ in case.blocks for x in n])
+        dr = (ctypes.c_double * (3 * nb))(*[float(x) for _, d in case.blocks for x in d])
+        qs = [np.ascontiguousarray(q, dtype=np.float64) for q in case.states]
+        qp = (ctypes.POINTER(ctypes.c_double) * nb)(*[q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for q in qs])
+        bc = (ctypes.c_int32 * max(1, 3 * len(case.bcs)))(*[int(x) for b in case.bcs for x in b])
+        conn = (abi.Connection * max(1, len(case.conns)))()
+        for i, (blk, rng, donor, drng, dtype) in enumerate(case.conns):
+            c = conn[i]
+            c.blk, c.donor = int(blk), int(donor)
+            for a in range(3):
+                c.range[a][0], c.range[a][1] = int(rng[a][0]), int(rng[a][1])
+                c.donor_range[a][0], c.donor_range[a][1] = int(drng[a][0]), int(drng[a][1])
+                c.donor_type[a] = int(dtype[a])
+        r = abi.Request()
+        r.struct_size = ctypes.sizeof(abi.Request)
+        r.nblocks = nb
+        r.cfg = ctypes.pointer(cfg)
+        r.nvert = nvert
+        r.dr = dr
+        r.q = qp
+        r.nbc = len(case.bcs)
+        r.bc = bc
+        r.nconn = len(case.conns)
+        r.conn = conn
+        r.steps = int(nsteps)
+        rid = ctypes.c_int64()
+        self._chk(self.lib.fvm_case_submit(self.h, ctypes.byref(r), ctypes.byref(rid)))
+        return rid.value
 
-    def admit(self, r: Request, now: float) -> bool:
-        """Place the request's blocks in the arena and upload its state; on a
-        fragmented arena (enough cells in total, no contiguous range) the case
-        is taken out again and the request stays queued."""
-        cid = self.s.add_case(r.case.config())
-        try:
-            r.case.apply(self.s, case_id=cid)
-        except FvmError as e:
-            if e.code != 3:  # FVM_ERR_NOMEM
-                raise
-            self.s.remove_case(cid)
-            return False
-        r.case_id = cid
-        r.remaining = r.nsteps
-        r.admitted = now
-        self.free -= r.cells
-        self.active.append(r)
-        return True
+    def poll(self, rid: int) -> dict:
+        st, status = ctypes.c_int(), ctypes.c_int()
+        done, t, lat = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        self._chk(self.lib.fvm_poll(self.h, rid, ctypes.byref(st), ctypes.byref(done), ctypes.byref(t),
+                                    ctypes.byref(lat), ctypes.byref(status)))
+        return {"state": st.value, "steps_done": done.value, "t": t.value, "latency_s": lat.value,
+                "status": status.value}
 
-    def retire(self, r: Request, now: float):
-        r.result = [self.s.get_state(b) for b in r.case.block_ids]
-        r.status = self.s.case_state(r.case_id)["status"]
-        self.s.remove_case(r.case_id)
-        self.free += r.cells
-        r.finished = now
-        self.active.remove(r)
+    def wait(self, rid: int, timeout: float = 600.0) -> int:
+        st = ctypes.c_int()
+        self._chk(self.lib.fvm_wait(self.h, rid, float(timeout), ctypes.byref(st)))
+        return st.value
+
+    def fetch(self, rid: int, case: cases.Case) -> list:
+        out = []
+        for b, (n, _) in enumerate(case.blocks):
+            q = np.empty((5, n[2], n[1], n[0]), dtype=np.float64)
+            self._chk(self.lib.fvm_fetch_state(self.h, rid, b, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+            out.append(q)
+        return out
+
+    def release(self, rid: int):
+        self._chk(self.lib.fvm_release(self.h, rid))
+
+    def stats(self) -> dict:
+        """Cells held by the running set now and at most so far, and the
+        numbers of running and queued requests (fvm_server_stats)."""
+        act, peak = ctypes.c_int64(), ctypes.c_int64()
+        run, que = ctypes.c_int(), ctypes.c_int()
+        self._chk(self.lib.fvm_server_stats(self.h, ctypes.byref(act), ctypes.byref(peak), ctypes.byref(run),
+                                            ctypes.byref(que)))
+        return {"active_cells": act.value, "peak_active_cells": peak.value, "running": run.value,
+                "queued": que.value}
 
     def run(self, stream: list[Request], clock=time.perf_counter, realtime: bool = True):
-        """Serve the stream; arrivals are honoured in wall-clock time when
-        `realtime`, else every request is present at t = 0. Returns stats."""
+        """Serve the stream: each request is submitted at its arrival time
+        (wall clock) when `realtime`, else all at t = 0; then every result is
+        awaited and read back. Time-to-solution is the library's own
+        submission-to-completion time. Returns stats."""
         pending = sorted(stream, key=lambda r: r.arrival)
         for r in pending:
             r.cells = self.cells_of(r.case)
             if r.cells > self.budget:
                 raise ValueError(f"request {r.rid} needs {r.cells} cells, more than the whole budget")
-        queue: list[Request] = []
-        done: list[Request] = []
         t0 = clock()
-        i = 0
-        while i < len(pending) or queue or self.active:
-            now = clock() - t0
-            while i < len(pending) and (not realtime or pending[i].arrival <= now):
-                queue.append(pending[i])
-                i += 1
-            while queue and self.fits(queue[0]):
-                if not self.admit(queue[0], now):
-                    break
-                queue.pop(0)
-            if not self.active:
-                if queue:
-                    raise RuntimeError("a queued request cannot be placed in the empty arena")
-                if i < len(pending) and realtime:
-                    time.sleep(max(0.0, min(0.002, pending[i].arrival - now)))
-                continue
-            k = min(min(r.remaining for r in self.active), self.chunk)
-            self.s.step(k)
-            self.steps_run += k
-            now = clock() - t0
-            for r in list(self.active):
-                r.remaining -= k
-                if r.remaining == 0:
-                    self.retire(r, clock() - t0)
-                    done.append(r)
-        makespan = clock() - t0
-        return summarize(done, makespan)
+        for r in pending:
+            if realtime:
+                wait = r.arrival - (clock() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+            r.submitted = clock() - t0
+            r.req_id = self.submit(r.case, r.nsteps)
+        for r in pending:
+            self.wait(r.req_id)
+            p = self.poll(r.req_id)
+            r.status = p["status"]
+            r.finished = r.submitted + p["latency_s"]
+            if not realtime:
+                r.arrival = 0.0
+            r.result = self.fetch(r.req_id, r.case)
+            self.release(r.req_id)
+        makespan = max((r.finished for r in pending), default=0.0)
+        return summarize(pending, makespan)
 
 
-def serve_one_at_a_time(stream: list[Request], clock=time.perf_counter, realtime: bool = True):
-    """Baseline: one engine per request, strictly in arrival order."""
+def serve_one_at_a_time(stream: list[Request], clock=time.perf_counter, realtime: bool = True, precision=None):
+    """Baseline: one engine per request, strictly in arrival order (each
+    request in its own precision form, or in `precision` when given)."""
     pending = sorted(stream, key=lambda r: r.arrival)
     done = []
     t0 = clock()
@@ -195,7 +268,8 @@ def serve_one_at_a_time(stream: list[Request], clock=time.perf_counter, realtime
         if realtime and r.arrival > now:
             time.sleep(r.arrival - now)
         r.admitted = clock() - t0
-        s = r.case.apply(Solver(r.case.config()))
+        over = {} if precision is None else {"precision": precision}
+        s = r.case.apply(Solver(r.case.config(**over)))
         s.step(r.nsteps)
         r.result = [s.get_state(b) for b in range(len(r.case.blocks))]
         r.status = s.case_state(0)["status"]

@@ -300,6 +300,91 @@ int fvm_residual_norms_noalloc(const double* rhs_dev, const int64_t nvert[3], do
 /* Release the context and its device memory. */
 int fvm_destroy(fvm_ctx* ctx);
 
+/* ---- serving: requests queued and run with continuous batching inside the
+ *      library. No counterpart in the reference, which runs one case per
+ *      process; a server runs the step loop of solve_process
+ *      (src/process/solver_sub.f90:196-207) for many cases at once.
+ * A worker thread owned by the server admits submitted requests first come,
+ * first served, while their arena cells (fvm_block_cells) fit the budget,
+ * advances every admitted case together (one persistent launch per scheme
+ * group and RK stage), and retires a case when its steps are done or its
+ * residual became NaN / diverged, keeping its final state in host memory
+ * until fvm_release. Cases with 3 and with 4 RK stages run in two engines
+ * whose steps overlap on the device; each engine reserves the whole budget
+ * when its first case arrives. A case's results equal its run alone bit for
+ * bit. Calls may come from any host thread; all device work happens on the
+ * worker thread, on the device current at fvm_server_create. */
+typedef struct fvm_server fvm_server;
+
+typedef struct fvm_server_config {
+  int32_t struct_size;      /* = sizeof(fvm_server_config)                      */
+  int32_t chunk_steps;      /* steps the running set advances between admissions */
+  int64_t budget_cells;     /* arena cells the running set may hold (HBM budget) */
+  int64_t max_active_cells; /* stop admitting once the running set holds this many
+                             * cells (0 = no cap; an empty set admits one request) */
+  int32_t max_queued;       /* fvm_case_submit returns FVM_ERR_BUSY beyond this many
+                             * waiting requests                                   */
+  int32_t pad_;
+} fvm_server_config;
+
+/* One block-to-block connection of a request, as fvm_connect takes it
+ * (block indices local to the request). */
+typedef struct fvm_connection {
+  int32_t blk, donor;
+  int64_t range[3][2];
+  int64_t donor_range[3][2];
+  int32_t donor_type[3];
+  int32_t pad_;
+} fvm_connection;
+
+/* A case to run: its configuration, blocks and initial state (layout of
+ * fvm_set_state), boundary kinds (bc[i] = {block, region 1..6, fvm_bc kind};
+ * regions not listed stay transmissive) and connections, and the number of
+ * time steps. Everything is copied by fvm_case_submit. */
+typedef struct fvm_request {
+  int32_t struct_size;        /* = sizeof(fvm_request)              */
+  int32_t nblocks;
+  const fvm_config* cfg;
+  const int64_t* nvert;       /* [nblocks][3]                       */
+  const double* dr;           /* [nblocks][3]                       */
+  const double* const* q;     /* [nblocks] host arrays              */
+  int32_t nbc, nconn;
+  const int32_t* bc;          /* [nbc][3]                           */
+  const fvm_connection* conn; /* [nconn]                            */
+  int64_t steps;              /* time steps to run, >= 1            */
+} fvm_request;
+
+enum fvm_request_state { FVM_REQ_QUEUED = 0, FVM_REQ_RUNNING = 1, FVM_REQ_DONE = 2, FVM_REQ_FAILED = 3 };
+
+/* Defaults: chunk 8 steps, budget 2^24 cells, no active cap, 1024 queued. */
+int fvm_server_config_default(fvm_server_config* cfg);
+int fvm_server_create(const fvm_server_config* cfg, fvm_server** out);
+/* Queue a request; *request_id identifies it. FVM_ERR_BUSY when max_queued
+ * requests are waiting, FVM_ERR_INVALID for a malformed request or one that
+ * needs more cells than the whole budget. A configuration the engine rejects
+ * fails the request later (state FVM_REQ_FAILED, status and message). */
+int fvm_case_submit(fvm_server* srv, const fvm_request* req, int64_t* request_id);
+/* State, steps done, physical time, time since submission (or from
+ * submission to completion once finished, in seconds) and status
+ * (FVM_OK or the error that failed it). Any output may be NULL.
+ * FVM_ERR_NOT_FOUND for an unknown or released id. */
+int fvm_poll(fvm_server* srv, int64_t request_id, int* state, int64_t* steps_done, double* t, double* latency_s,
+             int* status);
+/* Block until the request is done or failed, at most timeout_s seconds
+ * (FVM_ERR_TIMEOUT otherwise). */
+int fvm_wait(fvm_server* srv, int64_t request_id, double timeout_s, int* state);
+/* Copy the final state of block `blk` (request-local index) of a finished
+ * request into q (layout of fvm_get_state); FVM_ERR_BUSY before it finished. */
+int fvm_fetch_state(fvm_server* srv, int64_t request_id, int blk, double* q);
+/* Forget a finished request and free its host copy. */
+int fvm_release(fvm_server* srv, int64_t request_id);
+/* Cells the running set holds now and at most so far, running and queued
+ * request counts. Any output may be NULL. */
+int fvm_server_stats(fvm_server* srv, int64_t* active_cells, int64_t* peak_active_cells, int* running, int* queued);
+int fvm_server_last_error(fvm_server* srv, char* buf, size_t n);
+/* Stop the worker (running requests end as failed) and free everything. */
+int fvm_server_destroy(fvm_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

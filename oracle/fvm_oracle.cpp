@@ -755,18 +755,20 @@ void rk_update(orc_ctx* c, Block& b, int m, double dt) {
             else
               out = a3_1 * u0 + a3_2 * um + a3_3 * h * rm;
           } else {
+            // classic RK4, q0 folded into the accumulator (low storage: the
+            // last stage reads acc, not q0)
             double& acc = b.acc[r + e * rv];
             if (m == 1) {
-              acc = rm;
+              acc = u0 + h / 6.0 * rm;
               out = u0 + 0.5 * h * rm;
             } else if (m == 2) {
-              acc = acc + 2.0 * rm;
+              acc = acc + h / 3.0 * rm;
               out = u0 + 0.5 * h * rm;
             } else if (m == 3) {
-              acc = acc + 2.0 * rm;
+              acc = acc + h / 3.0 * rm;
               out = u0 + h * rm;
             } else {
-              out = u0 + h / 6.0 * (acc + rm);
+              out = acc + h / 6.0 * rm;
             }
           }
           b.q[g + e * gv] = out;

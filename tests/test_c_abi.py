@@ -102,3 +102,30 @@ def test_fortran_module_binds_header_functions():
         c_args = protos[cname].strip()
         n_c = 0 if c_args in ("", "void") else len(c_args.split(","))
         assert n_f == n_c, (cname, n_f, n_c)
+
+
+SERVE_SRC = os.path.join(ROOT, "tests", "c_driver", "fvm_c_serve.c")
+
+
+def build_serve(tmp_path) -> str:
+    exe = str(tmp_path / "fvm_c_serve")
+    cmd = ["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-O2", "-I", os.path.join(ROOT, "include"),
+           SERVE_SRC, "-o", exe, "-L", LIBDIR, "-lfvm3d", "-lm", f"-Wl,-rpath,{LIBDIR}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_serving_c_host_links(tmp_path):
+    build_serve(tmp_path)
+
+
+@pytest.mark.gpu
+def test_c_host_serves_three_requests(tmp_path):
+    # fvm_case_submit / fvm_wait / fvm_poll / fvm_fetch_state / fvm_release
+    # from C: an Euler RK3, an Euler RK4 (second engine) and a Navier-Stokes
+    # request served together, each bit-identical to its run alone
+    exe = build_serve(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "served 3 requests" in r.stdout

@@ -87,39 +87,85 @@ def test_reserved_budget_is_enforced():
     s.close()
 
 
+def _families_stream(n, seed, rate=1000.0):
+    # the served families of the three solver configurations (2D Riemann,
+    # 8-block vortex with RK4, Navier-Stokes TGV) and the batched blasts /
+    # shock tubes, small grids, a few steps each
+    fam = serving.config_families(precision=abi.PREC_FP32_FLUX, sizes=(12, 20))
+    mix = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(12, 24))
+    make = lambda rng, i: fam(rng, i) if i % 3 else mix(rng, i)  # noqa: E731
+    return serving.poisson_stream(n, rate=rate, seed=seed, make_case=make, steps=(3, 12))
+
+
 def test_server_results_same_alone_and_in_the_mix():
-    make = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(12, 24))
-    stream = serving.poisson_stream(8, rate=1000.0, seed=3, make_case=make, steps=(3, 12))
-    budget = 3 * max(sum(abi.block_cells(3, n) for n, _ in r.case.blocks) for r in stream)
+    stream = _families_stream(9, seed=3)
+    kinds = {r.case.name.split("_")[0] for r in stream}
+    assert {"riemann2d", "vortex", "tgv"} <= kinds, kinds
+    budget = 3 * max(sum(abi.block_cells(int(r.case.cfg.get("idimension", 3)), n) for n, _ in r.case.blocks)
+                     for r in stream)
     srv = serving.Server(budget_cells=budget, chunk=4)
     stats = srv.run(stream, realtime=False)
     srv.close()
-    assert stats["requests"] == 8 and stats["failed"] == 0
+    assert stats["requests"] == 9 and stats["failed"] == 0
     assert stats["p99_s"] >= stats["p50_s"] > 0
     for r in stream:
         ref = alone(r.case, r.nsteps)
         for got, want in zip(r.result, ref):
-            assert np.array_equal(got, want), f"request {r.rid}"
+            assert np.array_equal(got, want), f"request {r.rid} ({r.case.name})"
 
 
 def test_server_admission_cap():
-    make = serving.mixed_family(precision=abi.PREC_FP32_FLUX, sizes=(12, 24))
-    stream = serving.poisson_stream(8, rate=1000.0, seed=4, make_case=make, steps=(3, 12))
-    cells = [sum(abi.block_cells(3, n) for n, _ in r.case.blocks) for r in stream]
+    stream = _families_stream(8, seed=4)
+    srv0 = serving.Server(budget_cells=1 << 20)
+    cells = [srv0.cells_of(r.case) for r in stream]
+    srv0.close()
     cap = 2 * max(cells)
-    seen = []
-
-    class Probe(serving.Server):
-        def admit(self, r, now):
-            ok = super().admit(r, now)
-            seen.append(sum(a.cells for a in self.active))
-            return ok
-
-    srv = Probe(budget_cells=10 * max(cells), chunk=2, max_active_cells=cap)
+    srv = serving.Server(budget_cells=10 * max(cells), chunk=2, max_active_cells=cap)
     stats = srv.run(stream, realtime=False)
+    peak = srv.stats()["peak_active_cells"]
     srv.close()
     assert stats["requests"] == 8 and stats["failed"] == 0
-    assert max(seen) <= cap
+    assert 0 < peak <= cap
+
+
+def test_server_error_codes():
+    # FVM_ERR_NOT_FOUND for unknown / released ids, FVM_ERR_INVALID for a
+    # request above the whole budget, FVM_ERR_BUSY for a full queue and for
+    # reading an unfinished request
+    a = cases.taylor_green(N=24)
+    b = cases.blast((12, 12, 12), seed=0)
+    srv0 = serving.Server(budget_cells=1 << 20)
+    ca, cb = srv0.cells_of(a), srv0.cells_of(b)
+    srv0.close()
+    srv = serving.Server(budget_cells=ca, chunk=1, max_queued=1)
+    with pytest.raises(FvmError) as e:
+        srv.poll(777)
+    assert e.value.code == 10
+    with pytest.raises(FvmError) as e:
+        srv.submit(cases.taylor_green(N=40), 1)
+    assert e.value.code == 1
+    ra = srv.submit(a, 3000)
+    import time
+
+    t0 = time.time()
+    while srv.poll(ra)["state"] == abi.REQ_QUEUED and time.time() - t0 < 30:
+        time.sleep(0.001)
+    assert srv.poll(ra)["state"] == abi.REQ_RUNNING
+    assert cb <= ca
+    rb = srv.submit(b, 2)                      # waits: the running TGV holds the whole budget
+    with pytest.raises(FvmError) as e:
+        srv.submit(b, 2)                       # max_queued = 1
+    assert e.value.code == 9
+    with pytest.raises(FvmError) as e:
+        srv.fetch(ra, a)                       # still running
+    assert e.value.code == 9
+    assert srv.wait(ra) == abi.REQ_DONE and srv.wait(rb) == abi.REQ_DONE
+    assert srv.poll(ra)["steps_done"] == 3000
+    srv.release(ra)
+    with pytest.raises(FvmError) as e:
+        srv.poll(ra)
+    assert e.value.code == 10
+    srv.close()
 
 
 def test_navier_stokes_mixed_precisions_batched():
