@@ -28,6 +28,10 @@ module fvm3d_c
   public :: fvm_set_state, fvm_get_state, fvm_set_states, fvm_get_states, fvm_get_primitive, fvm_get_rhs
   public :: fvm_step, fvm_run, fvm_get_time, fvm_last_error
   public :: fvm_residual_norms, fvm_residual_norms_noalloc
+  public :: fvm_server_config_t, fvm_connection_t, fvm_request_t
+  public :: fvm_server_config_default, fvm_server_create, fvm_case_submit, fvm_poll, fvm_wait
+  public :: fvm_fetch_state, fvm_release, fvm_server_stats, fvm_server_last_error, fvm_server_destroy
+  public :: FVM_REQ_QUEUED, FVM_REQ_RUNNING, FVM_REQ_DONE, FVM_REQ_FAILED
   public :: FVM_OK, FVM_BC_TRANSMISSIVE, FVM_BC_PERIODIC, FVM_BC_CONNECTED
   public :: FVM_DT_FIXED, FVM_DT_CFL, FVM_DT_CFL_LOCAL
   public :: FVM_PREC_FP64_EXACT, FVM_PREC_FP64, FVM_PREC_FP32_FLUX
@@ -36,6 +40,7 @@ module fvm3d_c
   integer(c_int), parameter :: FVM_BC_TRANSMISSIVE = 0, FVM_BC_PERIODIC = 1, FVM_BC_CONNECTED = 2
   integer(c_int32_t), parameter :: FVM_DT_FIXED = 0, FVM_DT_CFL = 1, FVM_DT_CFL_LOCAL = 2
   integer(c_int32_t), parameter :: FVM_PREC_FP64_EXACT = 0, FVM_PREC_FP64 = 1, FVM_PREC_FP32_FLUX = 2
+  integer(c_int), parameter :: FVM_REQ_QUEUED = 0, FVM_REQ_RUNNING = 1, FVM_REQ_DONE = 2, FVM_REQ_FAILED = 3
 
   type, bind(c) :: fvm_config_t
     integer(c_int32_t) :: struct_size
@@ -58,6 +63,39 @@ module fvm3d_c
     real(c_double)     :: mu
     real(c_double)     :: prandtl
   end type fvm_config_t
+
+  ! struct fvm_server_config / fvm_connection / fvm_request (serving)
+  type, bind(c) :: fvm_server_config_t
+    integer(c_int32_t) :: struct_size
+    integer(c_int32_t) :: chunk_steps
+    integer(c_int64_t) :: budget_cells
+    integer(c_int64_t) :: max_active_cells
+    integer(c_int32_t) :: max_queued
+    integer(c_int32_t) :: pad_
+  end type fvm_server_config_t
+
+  type, bind(c) :: fvm_connection_t
+    integer(c_int32_t) :: blk, donor
+    integer(c_int64_t) :: range(2, 3)
+    integer(c_int64_t) :: donor_range(2, 3)
+    integer(c_int32_t) :: donor_type(3)
+    integer(c_int32_t) :: pad_
+  end type fvm_connection_t
+
+  ! nvert / dr: c_loc of (3, nblocks) arrays; q: c_loc of an array of
+  ! nblocks c_ptr, each c_loc(get_q()) of one block; bc: c_loc of (3, nbc)
+  type, bind(c) :: fvm_request_t
+    integer(c_int32_t) :: struct_size
+    integer(c_int32_t) :: nblocks
+    type(c_ptr)        :: cfg
+    type(c_ptr)        :: nvert
+    type(c_ptr)        :: dr
+    type(c_ptr)        :: q
+    integer(c_int32_t) :: nbc, nconn
+    type(c_ptr)        :: bc
+    type(c_ptr)        :: conn
+    integer(c_int64_t) :: steps
+  end type fvm_request_t
 
   interface
 
@@ -197,6 +235,77 @@ module fvm3d_c
       type(c_ptr), value :: rhs_dev, res_dev, stream
       integer(c_int64_t), intent(in) :: nvert(3)
     end function fvm_residual_norms_noalloc
+
+    ! ---- serving: many cases queued and run with continuous batching
+    integer(c_int) function fvm_server_config_default(cfg) bind(c, name="fvm_server_config_default")
+      import :: c_int, fvm_server_config_t
+      type(fvm_server_config_t), intent(out) :: cfg
+    end function fvm_server_config_default
+
+    integer(c_int) function fvm_server_create(cfg, srv) bind(c, name="fvm_server_create")
+      import :: c_int, c_ptr, fvm_server_config_t
+      type(fvm_server_config_t), intent(in) :: cfg
+      type(c_ptr), intent(out) :: srv
+    end function fvm_server_create
+
+    integer(c_int) function fvm_case_submit(srv, req, request_id) bind(c, name="fvm_case_submit")
+      import :: c_int, c_ptr, c_int64_t, fvm_request_t
+      type(c_ptr), value :: srv
+      type(fvm_request_t), intent(in) :: req
+      integer(c_int64_t), intent(out) :: request_id
+    end function fvm_case_submit
+
+    integer(c_int) function fvm_poll(srv, request_id, state, steps_done, t, latency_s, status) &
+        bind(c, name="fvm_poll")
+      import :: c_int, c_ptr, c_int64_t, c_double
+      type(c_ptr), value :: srv
+      integer(c_int64_t), value :: request_id
+      integer(c_int), intent(out) :: state, status
+      integer(c_int64_t), intent(out) :: steps_done
+      real(c_double), intent(out) :: t, latency_s
+    end function fvm_poll
+
+    integer(c_int) function fvm_wait(srv, request_id, timeout_s, state) bind(c, name="fvm_wait")
+      import :: c_int, c_ptr, c_int64_t, c_double
+      type(c_ptr), value :: srv
+      integer(c_int64_t), value :: request_id
+      real(c_double), value :: timeout_s
+      integer(c_int), intent(out) :: state
+    end function fvm_wait
+
+    integer(c_int) function fvm_fetch_state(srv, request_id, blk, q) bind(c, name="fvm_fetch_state")
+      import :: c_int, c_ptr, c_int64_t, c_double
+      type(c_ptr), value :: srv
+      integer(c_int64_t), value :: request_id
+      integer(c_int), value :: blk
+      real(c_double), intent(out) :: q(*)
+    end function fvm_fetch_state
+
+    integer(c_int) function fvm_release(srv, request_id) bind(c, name="fvm_release")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: srv
+      integer(c_int64_t), value :: request_id
+    end function fvm_release
+
+    integer(c_int) function fvm_server_stats(srv, active_cells, peak_active_cells, running, queued) &
+        bind(c, name="fvm_server_stats")
+      import :: c_int, c_ptr, c_int64_t
+      type(c_ptr), value :: srv
+      integer(c_int64_t), intent(out) :: active_cells, peak_active_cells
+      integer(c_int), intent(out) :: running, queued
+    end function fvm_server_stats
+
+    integer(c_int) function fvm_server_last_error(srv, buf, n) bind(c, name="fvm_server_last_error")
+      import :: c_int, c_ptr, c_char, c_size_t
+      type(c_ptr), value :: srv
+      character(kind=c_char), intent(out) :: buf(*)
+      integer(c_size_t), value :: n
+    end function fvm_server_last_error
+
+    integer(c_int) function fvm_server_destroy(srv) bind(c, name="fvm_server_destroy")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: srv
+    end function fvm_server_destroy
 
   end interface
 
