@@ -111,3 +111,30 @@ def test_last_error_message():
     with pytest.raises(FvmError) as e:
         Solver(reconstruct=abi.RECON_WCNS)
     assert "WCNS" in e.value.msg
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    # the ctypes mirrors of the header's structs have the C compiler's sizes
+    # and field offsets
+    src = tmp_path / "layout.c"
+    fields = {
+        "fvm_config": (abi.FvmConfig, ["struct_size", "store_rhs", "kappa", "prandtl"]),
+        "fvm_server_config": (abi.ServerConfig, ["chunk_steps", "budget_cells", "max_active_cells", "max_queued"]),
+        "fvm_connection": (abi.Connection, ["donor", "range", "donor_range", "donor_type"]),
+        "fvm_request": (abi.Request, ["nblocks", "cfg", "nvert", "dr", "q", "nbc", "nconn", "bc", "conn", "steps"]),
+    }
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "fvm3d.h"', "int main(void) {"]
+    for st, (_, fs) in fields.items():
+        lines.append(f'  printf("{st} size %zu\\n", sizeof({st}));')
+        for f in fs:
+            lines.append(f'  printf("{st} {f} %zu\\n", offsetof({st}, {f}));')
+    lines.append("  return 0;\n}")
+    src.write_text("\n".join(lines))
+    exe = str(tmp_path / "layout")
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", exe])
+    out = subprocess.check_output([exe]).decode().split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for st, (cls, fs) in fields.items():
+        assert got[(st, "size")] == ctypes.sizeof(cls), st
+        for f in fs:
+            assert got[(st, f)] == getattr(cls, f).offset, (st, f)
