@@ -133,7 +133,7 @@ def test_server_error_codes():
     # request above the whole budget, FVM_ERR_BUSY for a full queue and for
     # reading an unfinished request
     a = cases.taylor_green(N=24)
-    b = cases.blast((12, 12, 12), seed=0)
+    b = cases.blast((12, 12, 12), seed=0, limiter=abi.LIMITER_MINMOD, kappa=1.0 / 3.0)
     srv0 = serving.Server(budget_cells=1 << 20)
     ca, cb = srv0.cells_of(a), srv0.cells_of(b)
     srv0.close()
@@ -159,7 +159,8 @@ def test_server_error_codes():
     with pytest.raises(FvmError) as e:
         srv.fetch(ra, a)                       # still running
     assert e.value.code == 9
-    assert srv.wait(ra) == abi.REQ_DONE and srv.wait(rb) == abi.REQ_DONE
+    assert srv.wait(ra) == abi.REQ_DONE, srv.poll(ra)
+    assert srv.wait(rb) == abi.REQ_DONE, srv.poll(rb)
     assert srv.poll(ra)["steps_done"] == 3000
     srv.release(ra)
     with pytest.raises(FvmError) as e:
