@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include "fvm_aux.h"
+#include "fvm_finalize.cuh"
 #include "fvm_schemes.cuh"
 #include "fvm_types.h"
 #include "fvm_visc.cuh"
@@ -133,102 +134,13 @@ __global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const uns
 }
 
 // ---------------------------------------------------------------- finalize
-// One CTA per case, after the last stage of a step:
-// ClassIteration%reset_residual / compute_residual per block in block order /
-// update (class_iteration.f90, file-local 195-259), time += dt, the stop
-// checks of converged (:180-188) and the next step's dt.
+// One CTA per case, after the last stage of a step (finalize_case in
+// fvm_finalize.cuh).
 __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                                 const double* partials, int* counters, int ncounters) {
-  // one warp per block reduces its task partials (lanes stride the tasks,
-  // then a butterfly) and its lane 0 turns the sums into the block's squared
-  // norms; thread 0 folds the blocks in order, as the reference accumulates
-  // them (class_iteration.f90:195-259). The six folds are independent
-  // chains, so a block costs thread 0 one square root of latency.
-  constexpr int NW = 8;
-  __shared__ double red[NW][6];
-  __shared__ double redm[NW];
   pdl_wait();
   pdl_trigger();
-  const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const DevCase& C = cases[c];
-  if (c == 0)
-    for (int i = tid; i < ncounters; i += blockDim.x) counters[i] = 0;
-  if (C.nblocks == 0) return;  // removed case
-  double res[6] = {0, 0, 0, 0, 0, 0};
-  double wmax = 0.0;
-  for (int b0 = 0; b0 < C.nblocks; b0 += NW) {
-    const int bb = b0 + warp;
-    if (warp < NW && bb < C.nblocks) {
-      const DevBlock& B = blocks[case_blk[C.block0 + bb]];
-      // each lane loads kU partials before adding them (in a fixed order), so
-      // a block of many tasks costs one memory round trip per 32 * kU tasks
-      constexpr int kU = 8;
-      double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
-      for (int t = lane; t < B.ntask; t += 32 * kU) {
-        double q[kU][6];
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-          const int tt = t + 32 * u;
-          if (tt < B.ntask) {
-            const double* p = partials + (int64_t)(B.task0 + tt) * kPartStride;
-#pragma unroll
-            for (int v = 0; v < 6; ++v) q[u][v] = p[v];
-          } else {
-#pragma unroll
-            for (int v = 0; v < 6; ++v) q[u][v] = 0.0;  // adds nothing: same sums as task by task
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-#pragma unroll
-          for (int v = 0; v < 5; ++v) s[v] += q[u][v];
-          m = fmax(m, q[u][5]);
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], o);
-        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      }
-      if (lane == 0) {
-        const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
-        double res2_t = 0.0;
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const double r2 = s[v] / npt;
-          red[warp][v] = r2;
-          res2_t = res2_t + r2;
-        }
-        red[warp][5] = res2_t / 5.0;
-        redm[warp] = m;
-      }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      for (int w = 0; w < NW && b0 + w < C.nblocks; ++w) {
-#pragma unroll
-        for (int v = 0; v < 6; ++v) res[v] = sqrt(res[v] * res[v] + red[w][v]);
-        wmax = fmax(wmax, redm[w]);
-      }
-    }
-    __syncthreads();
-  }
-  if (tid == 0) {
-    DevCaseState& S = st[c];
-    S.step += 1;
-    S.t = S.t + S.dt;
-    S.dt_last = S.dt;
-    for (int e = 0; e < 6; ++e) S.res_abs[e] = res[e];
-    if (S.step == 1)
-      for (int e = 0; e < 6; ++e) S.res_abs0[e] = res[e];
-    for (int e = 0; e < 6; ++e) S.res_rel[e] = S.res_abs[e] / S.res_abs0[e];
-    if (isnan(res[5]))
-      S.status = 4;  // FVM_ERR_NONFINITE
-    else if (res[5] > 1.0E10)
-      S.status = 5;  // FVM_ERR_DIVERGED
-    S.dt = (C.timestep_set == 0) ? C.dt_fixed : C.cfl / wmax;
-  }
+  finalize_case(blockIdx.x, blocks, cases, case_blk, st, partials, counters, ncounters);
 }
 
 // ---------------------------------------------------------------- launchers

@@ -103,6 +103,10 @@ class Engine {
   // Tuning hooks (autotuner): force tile shape / z chunk of a case.
   int set_tuning(int case_id, int tile, int zchunk);
   int set_tail_split(int case_id, int split);
+  // Persistent 2D step kernel: -1 where eligible (the default), 0 never,
+  // 1 where eligible (the same as -1; kept for symmetry with the hook).
+  int set_fused_mode(int mode);
+  bool fused() const { return fused_; }
   // Mean device time of `reps` graph-launched steps (ms).
   int time_stage(int reps, float* ms);
 
@@ -135,6 +139,7 @@ class Engine {
   int plan();
   int build_graph();
   int enqueue_step(cudaEvent_t* evs, int nev, int* kinds, int* nlaunch);
+  StageArgs stage_args(int g, int m) const;
   void release();      // free everything (destruction)
   void invalidate() {  // topology changed: re-plan before the next use
     planned_ = false;
@@ -173,6 +178,10 @@ class Engine {
   int* d_dtmask_ = nullptr;           // cases whose dt prepare() recomputes
   int dtmask_cap_ = 0;
   bool drop_copies_ = false;          // test hook: tensor copies armed but not issued
+  int fused_mode_ = -1;               // persistent 2D step kernel: -1 auto, 0 off
+  bool fused_ = false;                // this plan runs steps with it
+  int fused_grid_ = 0;
+  unsigned int* d_bar_ = nullptr;     // its grid barrier (arrivals, generation)
   unsigned long long* d_casemax_ = nullptr;
   double* d_staging_ = nullptr;
   size_t staging_bytes_ = 0;

@@ -203,9 +203,21 @@ __device__ __forceinline__ int z_clamp(const BGeo& g, int z) {
   return z;
 }
 
+// COH: the loads must see writes made earlier in the same launch by other
+// CTAs (the persistent step kernel, whose stages run inside one launch):
+// L2-coherent loads instead of the read-only path, and plain copies instead
+// of asynchronous ones that may be served from this SM's L1.
+template <bool COH = false>
 __device__ __forceinline__ void ld5(const double* __restrict__ base, int64_t off, int64_t vs, double q[5]) {
 #pragma unroll
-  for (int v = 0; v < 5; ++v) q[v] = __ldg(base + off + v * vs);
+  for (int v = 0; v < 5; ++v) q[v] = COH ? __ldcg(base + off + v * vs) : __ldg(base + off + v * vs);
+}
+template <bool COH>
+__device__ __forceinline__ void cpy8(double* dst_smem, const double* src) {
+  if constexpr (COH)
+    *dst_smem = __ldcg(src);
+  else
+    __pipeline_memcpy_async(dst_smem, src, sizeof(double));
 }
 
 // Stencil value stored for reconstruction: conservative for WENO (the
@@ -319,10 +331,11 @@ __device__ __forceinline__ void plane_cell(int w, int& xx, int& yy) {
 }
 
 // ---------------------------------------------------------------- kernel
-template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, int MINB>
-__global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::NT,
-                                  (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 512 : 384) / (TX * TY)))
-    stage_kernel(const StageArgs a) {
+// One RK stage over the work list of `a`: the CTA takes tasks from the queue
+// until it is empty (or, with tensor copies, until a copy times out). The
+// body of stage_kernel, and of every stage of the persistent 2D step kernel.
+template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, bool COH = false>
+__device__ __forceinline__ void stage_run(const StageArgs& a) {
   using C = StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>;
   using R = typename C::R;
   constexpr bool EX = C::EX;
@@ -371,7 +384,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
     const Task T = a.tasks[ti];
     const DevBlock& B = a.blocks[T.blk];
     const DevCase& CS = a.cases[B.case_id];
-    const double dtg = a.cstate[B.case_id].dt;
+    const double dtg = COH ? __ldcg(&a.cstate[B.case_id].dt) : a.cstate[B.case_id].dt;
     const double* __restrict__ qin = B.q[a.rin];
     double* qout = B.q[a.rout];
     const double* q0p = B.q[a.rq0];
@@ -464,7 +477,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 #pragma unroll
       for (int s = 0; s < C::WIN; ++s) {
         double q[5];
-        ld5(qin, (int64_t)cxy + (int64_t)z_clamp(G, kstart - 1 + s) * G.sz, vs, q);
+        ld5<COH>(qin, (int64_t)cxy + (int64_t)z_clamp(G, kstart - 1 + s) * G.sz, vs, q);
         to_stencil<RECON, R, EX>(q, zw[s], gm1d, K.gm1);
       }
     } else {
@@ -474,7 +487,7 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
         if (lsp[sidx] >= 0) {
           double q[5];
           R s[5];
-          ld5(qin, (int64_t)lxy[sidx] + (int64_t)T.z0 * G.sz, vs, q);
+          ld5<COH>(qin, (int64_t)lxy[sidx] + (int64_t)T.z0 * G.sz, vs, q);
           to_stencil<RECON, R, EX>(q, s, gm1d, K.gm1);
 #pragma unroll
           for (int v = 0; v < 5; ++v) sP[v * PLANE + lsp[sidx]] = s[v];
@@ -514,9 +527,9 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
             if constexpr (C::PSM) {
               const int w = tid + sidx * NT;
 #pragma unroll
-              for (int v = 0; v < 5; ++v) __pipeline_memcpy_async(sX + v * C::NPL + w, src + v * vs, sizeof(double));
+              for (int v = 0; v < 5; ++v) cpy8<COH>(sX + v * C::NPL + w, src + v * vs);
             } else {
-              ld5(src, 0, vs, pre[sidx]);
+              ld5<COH>(src, 0, vs, pre[sidx]);
             }
           }
         }
@@ -526,9 +539,9 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
           const double* src = qin + (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz;
           if constexpr (C::PSM) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) __pipeline_memcpy_async(sZ + v * NC + tid, src + v * vs, sizeof(double));
+            for (int v = 0; v < 5; ++v) cpy8<COH>(sZ + v * NC + tid, src + v * vs);
           } else {
-            ld5(src, 0, vs, zpre);
+            ld5<COH>(src, 0, vs, zpre);
           }
         }
       }
@@ -552,9 +565,9 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
       } else if (do_xy && act) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          if (need_u0) __pipeline_memcpy_async(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs, sizeof(double));
-          if (need_um) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NC + tid, qin + off_k + v * vs, sizeof(double));
-          if (need_acc) __pipeline_memcpy_async(sQ + (1 * 5 + v) * NC + tid, accp + off_k + v * vs, sizeof(double));
+          if (need_u0) cpy8<COH>(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs);
+          if (need_um) cpy8<COH>(sQ + (1 * 5 + v) * NC + tid, qin + off_k + v * vs);
+          if (need_acc) cpy8<COH>(sQ + (1 * 5 + v) * NC + tid, accp + off_k + v * vs);
         }
         __pipeline_commit();
       }
@@ -1061,6 +1074,13 @@ __global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::
 
     if (a.last) cta_reduce_store<NT>(sS, s_red, a.partials + (int64_t)T.slot * kPartStride);
   }
+}
+
+template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>::NT,
+                                  (MINB > 0 ? MINB : (PREC == PREC_FP32 ? 512 : 384) / (TX * TY)))
+    stage_kernel(const StageArgs a) {
+  stage_run<RECON, FLUX, PREC, TB, DIM, TX, TY>(a);
 }
 
 }  // namespace fvm
