@@ -272,8 +272,24 @@ def product(args, dist: Dist):
     def gcs(ms):
         return ncells * stages * dist.world / (ms * 1e-3) / 1e9
 
-    def l1rho(a, b):
-        return float(np.mean([np.abs(a.get_state(i)[0] - b.get_state(i)[0]).mean() for i in range(nblk)]))
+    # L1 density difference between two precision forms after the same
+    # number of steps (warm-up + one timing window) from the same initial
+    # state: fresh contexts, since the timed runs take different step counts
+    l1_steps = args.warmup + args.steps
+    _rho = {}
+
+    def rho_after(f):
+        if f not in _rho:
+            r = runs[f]
+            s = fresh(r["prec"], *r["tiling"])
+            s.step(l1_steps)
+            _rho[f] = [s.get_state(i)[0] for i in range(nblk)]
+            s.close()
+        return _rho[f]
+
+    def l1rho(fa, fb):
+        a, b = rho_after(fa), rho_after(fb)
+        return float(np.mean([np.abs(a[i] - b[i]).mean() for i in range(nblk)]))
 
     # roofline of the dominant kernel (the fused stage): algorithmic bytes are
     # the FP64 state arrays each stage must read or write. RK4 with q0 folded
@@ -328,10 +344,11 @@ def product(args, dist: Dist):
                                if k in ("achieved", "frac", "traffic", "stage_ms_per_step")}
             ref = "fp64" if "fp64" in runs else ("exact" if "exact" in runs else None)
             if ref:
-                rec["l1_density_vs_" + ref] = sig(l1rho(r["s"], runs[ref]["s"]))
+                rec["l1_density_vs_" + ref] = sig(l1rho(f, ref))
+                rec["l1_steps"] = l1_steps
         out[{"fp64": "fp64_plain", "fp32": "fp32_flux", "exact": "fp64_exact"}[f]] = rec
     if "fp64" in runs and "exact" in runs and forms[0] == "fp64":
-        out["fp64_exact"]["l1_density_vs_fp64"] = sig(l1rho(runs["exact"]["s"], runs["fp64"]["s"]))
+        out["fp64_exact"]["l1_density_vs_fp64"] = sig(l1rho("exact", "fp64"))
     if "fp64" in runs and "fp32" in runs:
         out["vortex_fp32_over_fp64"] = sig(runs["fp64"]["ms"] / runs["fp32"]["ms"])
     for r in runs.values():
@@ -577,11 +594,21 @@ def riemann2d_leg(args):
                        ("fp64_exact", abi.PREC_FP64_EXACT)):
         if {"fp64": "fp64", "fp32_flux": "fp32", "fp64_exact": "exact"}[name] not in forms:
             continue
-        s = c.apply(Solver(c.config(precision=prec)))
-        s.step(3)
-        ms = statistics.median(timed_windows(s, steps, min_s=0.3))
-        out[name] = {"value": sig(c.ncells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms)}
-        s.close()
+        rec = {}
+        for mode in (1, 0):
+            s = Solver(c.config(precision=prec))
+            c.apply(s, states=False)
+            tuning.set_fused_step(s, mode)
+            c.apply_states(s)
+            s.step(3)
+            ms = statistics.median(timed_windows(s, steps, min_s=0.3))
+            if mode == 1:
+                rec = {"value": sig(c.ncells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms),
+                       "persistent_step_kernel": tuning.fused_step_active(s)}
+            else:
+                rec["launch_per_stage_ms_per_step"] = sig(ms)
+            s.close()
+        out[name] = rec
     if "fp64" in out and "fp32_flux" in out:
         out["fp32_over_fp64"] = sig(out["fp64"]["ms_per_step"] / out["fp32_flux"]["ms_per_step"])
     out["unit"] = UNIT

@@ -117,6 +117,7 @@ void Engine::release() {
   d_pairs_ = nullptr;
   d_counters_ = nullptr;
   d_casemax_ = nullptr;
+  cap_blocks_ = cap_cases_ = cap_case_blk_ = cap_tasks_ = cap_partials_ = cap_pairs_ = cap_counters_ = cap_casemax_ = 0;
   d_staging_ = nullptr;
   staging_bytes_ = 0;
   if (d_staging2_) cudaFree(d_staging2_);
@@ -296,6 +297,7 @@ int Engine::set_boundary(int blk, int region, int kind) {
     c.donor = blk;
     b.conns.push_back(c);
   }
+  cases[b.case_id].pairs_valid = false;
   invalidate();
   return FVM_OK;
 }
@@ -360,6 +362,7 @@ int Engine::connect(int blk, const int64_t range[3][2], int donor, const int64_t
   }
   b.bc[region - 1] = FVM_BC_CONNECTED;
   b.conns.push_back(c);
+  cases[b.case_id].pairs_valid = false;
   invalidate();
   return FVM_OK;
 }
@@ -636,6 +639,21 @@ int Engine::layout() {
   return FVM_OK;
 }
 
+// A device buffer of at least n elements (1 if n is 0), grown by half again
+// when it must grow; its contents are not kept.
+template <class T>
+static cudaError_t grow_buf(T** p, size_t* cap, size_t n) {
+  n = std::max<size_t>(n, 1);
+  if (*p && *cap >= n) return cudaSuccess;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const size_t c = n + n / 2;
+  const cudaError_t e = cudaMalloc(p, sizeof(T) * c);
+  if (e == cudaSuccess) *cap = c;
+  return e;
+}
+
 int Engine::plan() {
   destroy_graphs();
   if (!laid_out_) {
@@ -901,47 +919,64 @@ int Engine::plan() {
     }
   }
 
-  // -- ghost gather pairs (slab element offsets)
+  // -- ghost gather pairs (slab element offsets). A case's pairs depend only
+  //    on its own blocks (connections never cross cases) and their arena
+  //    offsets, which never change while the case lives, so they are built
+  //    once per case and reused by every later re-plan (the serving loop
+  //    re-plans at each admission and retirement).
   std::vector<int64_t> pairs;
+  std::vector<int64_t> cp;  // pairs of the case being built
   auto add_pair = [&](int bi, const int64_t x[3]) -> int {
     int64_t y[3] = {x[0], x[1], x[2]};
     int src_blk = -1;
     if (resolve(bi, y, &src_blk) != 0) return -1;
     const HBlock& b = blocks[bi];
     const HBlock& s = blocks[src_blk];
-    pairs.push_back(b.slab_off + b.org + x[0] + x[1] * b.sy + x[2] * b.sz);
-    pairs.push_back(s.slab_off + s.org + y[0] + y[1] * s.sy + y[2] * s.sz);
+    cp.push_back(b.slab_off + b.org + x[0] + x[1] * b.sy + x[2] * b.sz);
+    cp.push_back(s.slab_off + s.org + y[0] + y[1] * s.sy + y[2] * s.sz);
     return 0;
   };
-  for (int bi : live_blocks) {
-    const HBlock& b = blocks[bi];
-    for (const auto& c : b.conns)
-      for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
-        for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j)
-          for (int64_t i = c.range[0][0]; i <= c.range[0][1]; ++i) {
-            const int64_t x[3] = {i, j, k};
-            if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
-          }
-    if (cases[b.case_id].cfg.equation == FVM_EQ_NAVIER_STOKES) {
-      // layer-1 edge ghosts read by the viscous stencil where both regions are
-      // connected (a transmissive axis is clamped on load instead)
-      const int idim = cases[b.case_id].cfg.idimension;
-      for (int a = 0; a < idim; ++a)
-        for (int a2 = a + 1; a2 < idim; ++a2) {
-          const int c3 = 3 - a - a2;
-          for (int sa = 0; sa < 2; ++sa)
-            for (int sb = 0; sb < 2; ++sb) {
-              if (b.bc[2 * a + sa] == FVM_BC_TRANSMISSIVE || b.bc[2 * a2 + sb] == FVM_BC_TRANSMISSIVE) continue;
-              for (int64_t t = 0; t < b.n[c3]; ++t) {
-                int64_t x[3];
-                x[a] = sa ? b.n[a] : -1;
-                x[a2] = sb ? b.n[a2] : -1;
-                x[c3] = t;
-                if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "edge ghost without a real donor");
+  for (int ci : live_cases) {
+    HCase& hc = cases[ci];
+    std::vector<int64_t> key;
+    for (int bi : hc.blocks) key.push_back(blocks[bi].slab_off);
+    if (!hc.pairs_valid || key != hc.pairs_key) {
+      cp.clear();
+      for (int bi : hc.blocks) {
+        const HBlock& b = blocks[bi];
+        for (const auto& c : b.conns)
+          for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
+            for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j)
+              for (int64_t i = c.range[0][0]; i <= c.range[0][1]; ++i) {
+                const int64_t x[3] = {i, j, k};
+                if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
               }
+        if (hc.cfg.equation == FVM_EQ_NAVIER_STOKES) {
+          // layer-1 edge ghosts read by the viscous stencil where both regions
+          // are connected (a transmissive axis is clamped on load instead)
+          const int idim = hc.cfg.idimension;
+          for (int a = 0; a < idim; ++a)
+            for (int a2 = a + 1; a2 < idim; ++a2) {
+              const int c3 = 3 - a - a2;
+              for (int sa = 0; sa < 2; ++sa)
+                for (int sb = 0; sb < 2; ++sb) {
+                  if (b.bc[2 * a + sa] == FVM_BC_TRANSMISSIVE || b.bc[2 * a2 + sb] == FVM_BC_TRANSMISSIVE) continue;
+                  for (int64_t t = 0; t < b.n[c3]; ++t) {
+                    int64_t x[3];
+                    x[a] = sa ? b.n[a] : -1;
+                    x[a2] = sb ? b.n[a2] : -1;
+                    x[c3] = t;
+                    if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "edge ghost without a real donor");
+                  }
+                }
             }
         }
+      }
+      hc.pairs_cache = cp;
+      hc.pairs_key = key;
+      hc.pairs_valid = true;
     }
+    pairs.insert(pairs.end(), hc.pairs_cache.begin(), hc.pairs_cache.end());
   }
   npairs = (int64_t)pairs.size() / 2;
 
@@ -1028,26 +1063,22 @@ int Engine::plan() {
   // would take 344 GB in the 4 roles, twice the HBM): 8 bytes per pair.
   // Checked before the old descriptors are released.
   if (cap_ >= ((int64_t)1 << 31)) return fail(FVM_ERR_INVALID, "arena too large for 32-bit ghost offsets");
-  // Every pointer is cleared as it is freed, so an allocation failure below
-  // (CK returns early) leaves null members, never freed addresses that the
-  // next plan() or the destructor would free a second time.
-  void** old[] = {(void**)&d_blocks_, (void**)&d_cases_,    (void**)&d_case_blk_, (void**)&d_tasks_,
-                  (void**)&d_partials_, (void**)&d_pairs_, (void**)&d_counters_, (void**)&d_casemax_};
-  for (void** p : old) {
-    if (*p) cudaFree(*p);
-    *p = nullptr;
-  }
+  // Descriptor buffers grow (never shrink) across re-plans, so admitting or
+  // retiring a case between steps costs no cudaFree / cudaMalloc (which
+  // would synchronise the device) unless a buffer must grow; a growth frees
+  // the old buffer and clears its pointer first, so a failed allocation
+  // leaves a null member, never a freed address.
   planned_ = false;
-  CK(cudaMalloc(&d_blocks_, sizeof(DevBlock) * blocks.size()));
-  CK(cudaMalloc(&d_cases_, sizeof(DevCase) * cases.size()));
-  CK(cudaMalloc(&d_case_blk_, sizeof(int) * std::max<size_t>(1, case_blk.size())));
-  CK(cudaMalloc(&d_tasks_, sizeof(Task) * std::max<size_t>(1, tasks.size())));
-  CK(cudaMalloc(&d_partials_, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size())));
   std::vector<int32_t> pairs32(pairs.begin(), pairs.end());
-  CK(cudaMalloc(&d_pairs_, sizeof(int32_t) * std::max<size_t>(2, pairs32.size())));
   ncounters_ = max_stages_ * (int)groups.size();
-  CK(cudaMalloc(&d_counters_, sizeof(int) * std::max(1, ncounters_)));
-  CK(cudaMalloc(&d_casemax_, sizeof(unsigned long long) * cases.size()));
+  CK(grow_buf(&d_blocks_, &cap_blocks_, blocks.size()));
+  CK(grow_buf(&d_cases_, &cap_cases_, cases.size()));
+  CK(grow_buf(&d_case_blk_, &cap_case_blk_, case_blk.size()));
+  CK(grow_buf(&d_tasks_, &cap_tasks_, tasks.size()));
+  CK(grow_buf(&d_partials_, &cap_partials_, kPartStride * std::max<size_t>(1, tasks.size())));
+  CK(grow_buf(&d_pairs_, &cap_pairs_, std::max<size_t>(2, pairs32.size())));
+  CK(grow_buf(&d_counters_, &cap_counters_, (size_t)std::max(1, ncounters_)));
+  CK(grow_buf(&d_casemax_, &cap_casemax_, cases.size()));
   CK(cudaMemcpyAsync(d_blocks_, h_dblocks_.data(), sizeof(DevBlock) * blocks.size(), cudaMemcpyHostToDevice, stream));
   CK(cudaMemcpyAsync(d_cases_, hcases.data(), sizeof(DevCase) * cases.size(), cudaMemcpyHostToDevice, stream));
   if (!case_blk.empty())
@@ -1563,6 +1594,21 @@ int Engine::read_case_state(int case_id, DevCaseState* out) {
     CK(cudaStreamSynchronize(stream));
     return fail(FVM_ERR_TIMEOUT, err == 2 ? "a grid barrier of the persistent step kernel waited more than 1 s"
                                           : "a stage kernel's tensor copy did not arrive within 1 s");
+  }
+  return FVM_OK;
+}
+
+int Engine::read_all_case_states(std::vector<DevCaseState>* out) {
+  out->assign(std::max(0, state_cap_), DevCaseState());
+  if (!d_state_ || state_cap_ == 0) return FVM_OK;
+  CK(cudaMemcpyAsync(out->data(), d_state_, sizeof(DevCaseState) * state_cap_, cudaMemcpyDeviceToHost, stream));
+  int32_t err = 0;
+  if (d_err_) CK(cudaMemcpyAsync(&err, d_err_, sizeof err, cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  if (err) {
+    CK(cudaMemsetAsync(d_err_, 0, sizeof(int32_t), stream));
+    CK(cudaStreamSynchronize(stream));
+    return fail(FVM_ERR_TIMEOUT, "a bounded wait of a kernel ran out (tensor copy or grid barrier)");
   }
   return FVM_OK;
 }

@@ -60,6 +60,10 @@ struct HCase {
   int tile = -1;        // forced tile (autotuner result), -1 = heuristic
   int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model over the case's group
   int tail_split = 1;   // pieces each task of the last, partial queue round is cut into (1 = none)
+  // ghost gather pairs of this case, valid while its blocks keep the arena
+  // offsets in pairs_key (topology edits clear pairs_valid)
+  std::vector<int64_t> pairs_cache, pairs_key;
+  bool pairs_valid = false;
 };
 
 struct Group {
@@ -93,6 +97,8 @@ class Engine {
   int get_rhs(int blk, double* rhs);
   int step(int nsteps);
   int read_case_state(int case_id, DevCaseState* out);
+  // every case's state in one copy (index = case id; fresh cases hold zeros)
+  int read_all_case_states(std::vector<DevCaseState>* out);
   // true once the case's device state exists (read_case_state would succeed)
   bool has_case_state(int case_id) const {
     return live_case(case_id) && d_state_ && case_id < state_cap_ && !cases[case_id].fresh;
@@ -183,6 +189,9 @@ class Engine {
   int fused_grid_ = 0;
   unsigned int* d_bar_ = nullptr;     // its grid barrier (arrivals, generation)
   unsigned long long* d_casemax_ = nullptr;
+  // element capacities of the descriptor buffers above (grown, never shrunk)
+  size_t cap_blocks_ = 0, cap_cases_ = 0, cap_case_blk_ = 0, cap_tasks_ = 0, cap_partials_ = 0, cap_pairs_ = 0,
+         cap_counters_ = 0, cap_casemax_ = 0;
   double* d_staging_ = nullptr;
   size_t staging_bytes_ = 0;
   double* d_staging2_ = nullptr;      // second staging buffer of set_states / get_states

@@ -241,7 +241,11 @@ void worker_main(fvm_server* s) {
         rc[e] = FVM_ERR_CUDA;
         s->eng[e]->err = cudaGetErrorString(cudaGetLastError());
       }
-    // -- progress, and retire what is done or failed
+    // -- progress (one copy of every case state per engine), and retire
+    //    what is done or failed
+    std::vector<fvm::DevCaseState> states[2];
+    for (int e = 0; e < 2; ++e)
+      if (used[e] && !rc[e]) rc[e] = s->eng[e]->read_all_case_states(&states[e]);
     std::vector<std::shared_ptr<Req>> keep;
     for (auto& r : s->active) {
       fvm::Engine* en = s->eng[r->engine].get();
@@ -250,7 +254,12 @@ void worker_main(fvm_server* s) {
         continue;
       }
       fvm::DevCaseState cs;
-      const int rr = en->read_case_state(r->case_id, &cs);
+      std::memset(&cs, 0, sizeof cs);
+      int rr = FVM_OK;
+      if (r->case_id < (int)states[r->engine].size() && en->has_case_state(r->case_id))
+        cs = states[r->engine][r->case_id];
+      else
+        rr = en->read_case_state(r->case_id, &cs);
       {
         std::lock_guard<std::mutex> lk(s->mu);
         r->steps_done += k;

@@ -82,8 +82,13 @@ class Case:
         for blk, rng, donor, drng, dtype in self.conns:
             target.connect(ids[blk], rng, ids[donor], drng, dtype)
         if states:
-            for b, q in enumerate(self.states):
-                target.set_state(ids[b], q)
+            self.apply_states(target)
+        return target
+
+    def apply_states(self, target):
+        """Upload the initial states to the blocks apply() created."""
+        for b, q in enumerate(self.states):
+            target.set_state(self.block_ids[b], q)
         return target
 
 
