@@ -594,21 +594,11 @@ def riemann2d_leg(args):
                        ("fp64_exact", abi.PREC_FP64_EXACT)):
         if {"fp64": "fp64", "fp32_flux": "fp32", "fp64_exact": "exact"}[name] not in forms:
             continue
-        rec = {}
-        for mode in (1, 0):
-            s = Solver(c.config(precision=prec))
-            c.apply(s, states=False)
-            tuning.set_fused_step(s, mode)
-            c.apply_states(s)
-            s.step(3)
-            ms = statistics.median(timed_windows(s, steps, min_s=0.3))
-            if mode == 1:
-                rec = {"value": sig(c.ncells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms),
-                       "persistent_step_kernel": tuning.fused_step_active(s)}
-            else:
-                rec["launch_per_stage_ms_per_step"] = sig(ms)
-            s.close()
-        out[name] = rec
+        s = c.apply(Solver(c.config(precision=prec)))
+        s.step(3)
+        ms = statistics.median(timed_windows(s, steps, min_s=0.3))
+        out[name] = {"value": sig(c.ncells * 3 / (ms * 1e-3) / 1e9), "ms_per_step": sig(ms)}
+        s.close()
     if "fp64" in out and "fp32_flux" in out:
         out["fp32_over_fp64"] = sig(out["fp64"]["ms_per_step"] / out["fp32_flux"]["ms_per_step"])
     out["unit"] = UNIT

@@ -68,9 +68,6 @@ struct StageKernelInfo {
   // tensor-map prefetch: the plane box is box_w x box_h cells (x, y), the z
   // box tx x ty; the kernel expects StageArgs::tmap (0 = no tensor maps)
   int tma = 0, box_w = 0, box_h = 0, halo = 0;
-  // the persistent 2D step kernel of the same scheme and tile (cooperative
-  // launch, Step2DArgs; 2D instantiations only, else null)
-  const void* step2d = nullptr;
 };
 
 // Tile shapes compiled for every scheme (index -> TX x TY, minimum resident

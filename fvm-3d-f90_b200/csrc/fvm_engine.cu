@@ -128,9 +128,6 @@ void Engine::release() {
   d_tmap_.clear();
   if (d_err_) cudaFree(d_err_);
   d_err_ = nullptr;
-  if (d_bar_) cudaFree(d_bar_);
-  d_bar_ = nullptr;
-  fused_ = false;
   if (d_dtmask_) cudaFree(d_dtmask_);
   d_dtmask_ = nullptr;
   dtmask_cap_ = 0;
@@ -1133,38 +1130,7 @@ int Engine::plan() {
   planned_ = true;
   prepared_ = false;
 
-  // The persistent 2D step kernel takes over whole steps of a single-group
-  // 2D Euler engine without connected regions (no ghost gather, no viscous
-  // launch): one cooperative launch per fvm_step call instead of a launch
-  // per stage, results bit-identical (fvm_tune_set_fused_step switches it).
-  fused_ = false;
-  bool visc = false;
-  for (int li = 0; li < 6; ++li) visc = visc || vlist_n_[li] > 0;
-  if (fused_mode_ != 0 && groups.size() == 1 && groups[0].dim == 2 && groups[0].k.step2d && npairs == 0 && !visc) {
-    const Group& G = groups[0];
-    int coop = 0, occ = 0;
-    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
-    CK(cudaFuncSetAttribute(G.k.step2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.k.smem));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, G.k.step2d, G.k.threads, G.k.smem));
-    if (coop && occ >= 1) {
-      if (!d_bar_) CK(cudaMalloc(&d_bar_, 2 * sizeof(unsigned int)));
-      fused_grid_ = std::max(1, std::min(occ * num_sms, G.ntasks));
-      fused_ = true;
-      kernel_launches_per_step = 1;  // one launch per fvm_step call, whatever its step count
-      return FVM_OK;
-    }
-  }
   return build_graph();
-}
-
-int Engine::set_fused_mode(int mode) {
-  if (mode < -1 || mode > 1) return fail(FVM_ERR_INVALID, "fused step mode must be -1, 0 or 1");
-  if (fused_mode_ != mode) {
-    fused_mode_ = mode;
-    planned_ = false;
-    prepared_ = false;
-  }
-  return FVM_OK;
 }
 
 // Enqueue one full time step on `stream`: per stage the optional viscous
@@ -1270,42 +1236,9 @@ void Engine::destroy_graphs() {
   graphm_ = nullptr;
 }
 
-// nsteps steps: one cooperative launch of the persistent 2D step kernel, or
-// runs of kMultiSteps from the multi-step graph and the rest one by one.
+// nsteps steps: runs of kMultiSteps from the multi-step graph, the rest one
+// by one.
 cudaError_t Engine::launch_steps(int nsteps) {
-  if (fused_) {
-    if (nsteps <= 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(d_bar_, 0, 2 * sizeof(unsigned int), stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_counters_, 0, sizeof(int) * std::max(1, ncounters_), stream);
-    if (e != cudaSuccess) return e;
-    const Group& G = groups[0];
-    Step2DArgs a;
-    std::memset(&a, 0, sizeof a);
-    for (int m = 1; m <= max_stages_; ++m) a.st[m - 1] = stage_args(0, m);
-    a.nstages = max_stages_;
-    a.nsteps = nsteps;
-    a.blocks = d_blocks_;
-    a.cases = d_cases_;
-    a.case_blk = d_case_blk_;
-    a.state = d_state_;
-    a.ncases = (int)cases.size();
-    a.ncounters = ncounters_;
-    a.counters = d_counters_;
-    a.bar = d_bar_;
-    a.err = d_err_;
-    void* args[] = {&a};
-    cudaLaunchConfig_t cfg{};
-    cudaLaunchAttribute attr[1]{};
-    cfg.gridDim = dim3(fused_grid_);
-    cfg.blockDim = dim3(G.k.threads);
-    cfg.dynamicSmemBytes = G.k.smem;
-    cfg.stream = stream;
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelExC(&cfg, G.k.step2d, args);
-  }
   int n = nsteps;
   for (; gexecm_ && n >= kMultiSteps; n -= kMultiSteps) {
     cudaError_t e = cudaGraphLaunch(gexecm_, stream);
@@ -1592,8 +1525,7 @@ int Engine::read_case_state(int case_id, DevCaseState* out) {
     // reported once; the context stays usable (the state of this step is not)
     CK(cudaMemsetAsync(d_err_, 0, sizeof(int32_t), stream));
     CK(cudaStreamSynchronize(stream));
-    return fail(FVM_ERR_TIMEOUT, err == 2 ? "a grid barrier of the persistent step kernel waited more than 1 s"
-                                          : "a stage kernel's tensor copy did not arrive within 1 s");
+    return fail(FVM_ERR_TIMEOUT, "a stage kernel's tensor copy did not arrive within 1 s");
   }
   return FVM_OK;
 }
@@ -1608,7 +1540,7 @@ int Engine::read_all_case_states(std::vector<DevCaseState>* out) {
   if (err) {
     CK(cudaMemsetAsync(d_err_, 0, sizeof(int32_t), stream));
     CK(cudaStreamSynchronize(stream));
-    return fail(FVM_ERR_TIMEOUT, "a bounded wait of a kernel ran out (tensor copy or grid barrier)");
+    return fail(FVM_ERR_TIMEOUT, "a stage kernel's tensor copy did not arrive within 1 s");
   }
   return FVM_OK;
 }
@@ -1881,19 +1813,6 @@ int fvm_tune_set(fvm_ctx* ctx, int case_id, int tile, int zchunk) {
 int fvm_tune_set_tail_split(fvm_ctx* ctx, int case_id, int split) {
   if (!ctx) return FVM_ERR_INVALID;
   return ctx->eng.set_tail_split(case_id, split);
-}
-
-int fvm_tune_set_fused_step(fvm_ctx* ctx, int mode) {
-  if (!ctx) return FVM_ERR_INVALID;
-  return ctx->eng.set_fused_mode(mode);
-}
-
-int fvm_fused_step_active(fvm_ctx* ctx, int* active) {
-  if (!ctx || !active) return FVM_ERR_INVALID;
-  int rc = ctx->eng.ensure_planned();
-  if (rc) return rc;
-  *active = ctx->eng.fused() ? 1 : 0;
-  return FVM_OK;
 }
 
 int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step) {

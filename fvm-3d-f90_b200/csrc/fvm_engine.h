@@ -109,10 +109,6 @@ class Engine {
   // Tuning hooks (autotuner): force tile shape / z chunk of a case.
   int set_tuning(int case_id, int tile, int zchunk);
   int set_tail_split(int case_id, int split);
-  // Persistent 2D step kernel: -1 where eligible (the default), 0 never,
-  // 1 where eligible (the same as -1; kept for symmetry with the hook).
-  int set_fused_mode(int mode);
-  bool fused() const { return fused_; }
   // Mean device time of `reps` graph-launched steps (ms).
   int time_stage(int reps, float* ms);
 
@@ -184,10 +180,6 @@ class Engine {
   int* d_dtmask_ = nullptr;           // cases whose dt prepare() recomputes
   int dtmask_cap_ = 0;
   bool drop_copies_ = false;          // test hook: tensor copies armed but not issued
-  int fused_mode_ = -1;               // persistent 2D step kernel: -1 auto, 0 off
-  bool fused_ = false;                // this plan runs steps with it
-  int fused_grid_ = 0;
-  unsigned int* d_bar_ = nullptr;     // its grid barrier (arrivals, generation)
   unsigned long long* d_casemax_ = nullptr;
   // element capacities of the descriptor buffers above (grown, never shrunk)
   size_t cap_blocks_ = 0, cap_cases_ = 0, cap_case_blk_ = 0, cap_tasks_ = 0, cap_partials_ = 0, cap_pairs_ = 0,

@@ -2,10 +2,9 @@
 // device function: ClassIteration%reset_residual / compute_residual per
 // block in block order / update (class_iteration.f90, file-local 195-259),
 // time += dt, the stop checks of converged (:180-188) and the next step's dt.
-// Run by finalize_kernel (one CTA per case) and by the persistent 2D step
-// kernel. Every FP64 operation is an explicitly rounded intrinsic, so the
-// result is the same whatever contraction or fast-math flags the including
-// translation unit is compiled with.
+// Run by finalize_kernel, one CTA per case. Every FP64 operation is an
+// explicitly rounded intrinsic, so the result does not depend on the
+// contraction or fast-math flags of the including translation unit.
 #pragma once
 #include <cuda_runtime.h>
 

@@ -174,16 +174,30 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
   }
   return false;
 }
-// Error path: wait up to 200 ms for the last armed phase of b (parity
-// `parity`) to complete, so no copy is left writing into shared memory.
-// Returns at once when that phase has already completed (or was never armed
-// since the previous completed wait).
+// Error path: wait up to 200 ms for the phase `parity` of b to complete, so
+// no copy is left writing into shared memory. Returns at once when that
+// phase has already completed.
 __device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
   const uint64_t t0 = global_ns();
   for (int i = 0; i < (1 << 24); ++i) {
     if (mbar_try_wait(b, parity)) return;
     if (global_ns() - t0 > 200000000ull) return;
   }
+}
+// Leaving the stage after a tensor copy timed out (the whole CTA, after a
+// barrier that published the outcome): thread 0 reports it and waits,
+// bounded, for every copy of this plane still in flight (the phases not yet
+// waited for: the operand boxes unless they already arrived, the z box if
+// issued, the plane box if issued), so none writes into the shared memory of
+// an exited CTA.
+__device__ __forceinline__ void leave_after_timeout(int tid, int32_t* err, uint64_t* mbar, uint32_t ph_p, uint32_t ph_z,
+                                                    uint32_t ph_q, bool plane_issued, bool z_issued,
+                                                    bool operands_pending) {
+  if (tid != 0) return;
+  atomicExch(err, 1);
+  if (operands_pending) mbar_drain(&mbar[2], ph_q);
+  if (z_issued) mbar_drain(&mbar[1], ph_z);
+  if (plane_issued) mbar_drain(&mbar[0], ph_p);
 }
 // 4D tiled tensor copy global -> this CTA's shared memory, completing on b.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -203,21 +217,12 @@ __device__ __forceinline__ int z_clamp(const BGeo& g, int z) {
   return z;
 }
 
-// COH: the loads must see writes made earlier in the same launch by other
-// CTAs (the persistent step kernel, whose stages run inside one launch):
-// L2-coherent loads instead of the read-only path, and plain copies instead
-// of asynchronous ones that may be served from this SM's L1.
-template <bool COH = false>
 __device__ __forceinline__ void ld5(const double* __restrict__ base, int64_t off, int64_t vs, double q[5]) {
 #pragma unroll
-  for (int v = 0; v < 5; ++v) q[v] = COH ? __ldcg(base + off + v * vs) : __ldg(base + off + v * vs);
+  for (int v = 0; v < 5; ++v) q[v] = __ldg(base + off + v * vs);
 }
-template <bool COH>
 __device__ __forceinline__ void cpy8(double* dst_smem, const double* src) {
-  if constexpr (COH)
-    *dst_smem = __ldcg(src);
-  else
-    __pipeline_memcpy_async(dst_smem, src, sizeof(double));
+  __pipeline_memcpy_async(dst_smem, src, sizeof(double));
 }
 
 // Stencil value stored for reconstruction: conservative for WENO (the
@@ -332,9 +337,8 @@ __device__ __forceinline__ void plane_cell(int w, int& xx, int& yy) {
 
 // ---------------------------------------------------------------- kernel
 // One RK stage over the work list of `a`: the CTA takes tasks from the queue
-// until it is empty (or, with tensor copies, until a copy times out). The
-// body of stage_kernel, and of every stage of the persistent 2D step kernel.
-template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY, bool COH = false>
+// until it is empty (or, with tensor copies, until a copy times out).
+template <int RECON, int FLUX, int PREC, bool TB, int DIM, int TX, int TY>
 __device__ __forceinline__ void stage_run(const StageArgs& a) {
   using C = StageCfg<RECON, FLUX, PREC, TB, DIM, TX, TY>;
   using R = typename C::R;
@@ -355,6 +359,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
   __shared__ double s_red[6 * (NT / 32)];
   __shared__ int s_task;
   __shared__ __align__(8) uint64_t s_mbar[3];  // TMA: plane box, z box, RK operands
+  __shared__ int s_fail_q, s_fail_zp;            // TMA: thread 0's wait outcomes (1 = timed out)
   uint32_t ph_p = 0, ph_z = 0, ph_q = 0;       // TMA: expected phase parity of each mbarrier
 
   const int tid = threadIdx.x;
@@ -384,7 +389,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
     const Task T = a.tasks[ti];
     const DevBlock& B = a.blocks[T.blk];
     const DevCase& CS = a.cases[B.case_id];
-    const double dtg = COH ? __ldcg(&a.cstate[B.case_id].dt) : a.cstate[B.case_id].dt;
+    const double dtg = a.cstate[B.case_id].dt;
     const double* __restrict__ qin = B.q[a.rin];
     double* qout = B.q[a.rout];
     const double* q0p = B.q[a.rq0];
@@ -477,7 +482,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
 #pragma unroll
       for (int s = 0; s < C::WIN; ++s) {
         double q[5];
-        ld5<COH>(qin, (int64_t)cxy + (int64_t)z_clamp(G, kstart - 1 + s) * G.sz, vs, q);
+        ld5(qin, (int64_t)cxy + (int64_t)z_clamp(G, kstart - 1 + s) * G.sz, vs, q);
         to_stencil<RECON, R, EX>(q, zw[s], gm1d, K.gm1);
       }
     } else {
@@ -487,7 +492,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
         if (lsp[sidx] >= 0) {
           double q[5];
           R s[5];
-          ld5<COH>(qin, (int64_t)lxy[sidx] + (int64_t)T.z0 * G.sz, vs, q);
+          ld5(qin, (int64_t)lxy[sidx] + (int64_t)T.z0 * G.sz, vs, q);
           to_stencil<RECON, R, EX>(q, s, gm1d, K.gm1);
 #pragma unroll
           for (int v = 0; v < 5; ++v) sP[v * PLANE + lsp[sidx]] = s[v];
@@ -527,9 +532,9 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             if constexpr (C::PSM) {
               const int w = tid + sidx * NT;
 #pragma unroll
-              for (int v = 0; v < 5; ++v) cpy8<COH>(sX + v * C::NPL + w, src + v * vs);
+              for (int v = 0; v < 5; ++v) cpy8(sX + v * C::NPL + w, src + v * vs);
             } else {
-              ld5<COH>(src, 0, vs, pre[sidx]);
+              ld5(src, 0, vs, pre[sidx]);
             }
           }
         }
@@ -539,9 +544,9 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           const double* src = qin + (int64_t)cxy + (int64_t)z_clamp(G, k + H + 1) * G.sz;
           if constexpr (C::PSM) {
 #pragma unroll
-            for (int v = 0; v < 5; ++v) cpy8<COH>(sZ + v * NC + tid, src + v * vs);
+            for (int v = 0; v < 5; ++v) cpy8(sZ + v * NC + tid, src + v * vs);
           } else {
-            ld5<COH>(src, 0, vs, zpre);
+            ld5(src, 0, vs, zpre);
           }
         }
       }
@@ -565,9 +570,9 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       } else if (do_xy && act) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          if (need_u0) cpy8<COH>(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs);
-          if (need_um) cpy8<COH>(sQ + (1 * 5 + v) * NC + tid, qin + off_k + v * vs);
-          if (need_acc) cpy8<COH>(sQ + (1 * 5 + v) * NC + tid, accp + off_k + v * vs);
+          if (need_u0) cpy8(sQ + (0 * 5 + v) * NC + tid, q0p + off_k + v * vs);
+          if (need_um) cpy8(sQ + (1 * 5 + v) * NC + tid, qin + off_k + v * vs);
+          if (need_acc) cpy8(sQ + (1 * 5 + v) * NC + tid, accp + off_k + v * vs);
         }
         __pipeline_commit();
       }
@@ -879,20 +884,26 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
         }
       }
+      // Tensor copies: thread 0 alone waits (bounded) for this plane's
+      // operand boxes and posts the outcome before the barrier, so the whole
+      // CTA takes the same decision after it without another barrier; the
+      // other threads then observe the completed phase themselves (at once).
+      if constexpr (C::TMA)
+        if (tid == 0 && do_xy) s_fail_q = mbar_wait(&s_mbar[2], ph_q) ? 0 : 1;
       __syncthreads();
 
       // ---- phase C: rhs, RK update, reductions -------------------------------
-      // fail: a tensor copy of this plane did not arrive in time (seen by this
-      // thread); the CTA decides together at the end of the plane
-      bool fail = false;
       if constexpr (C::TMA) {
-        // every thread waits for the operand boxes issued at the top of this plane
         if (do_xy) {
-          fail = !mbar_wait(&s_mbar[2], ph_q);
+          if (s_fail_q) {
+            leave_after_timeout(tid, a.err, s_mbar, ph_p, ph_z, ph_q, more_xy, more, true);
+            return;
+          }
+          mbar_wait(&s_mbar[2], ph_q);
           ph_q ^= 1;
         }
       }
-      if (do_xy && act && !fail) {
+      if (do_xy && act) {
         constexpr int NF = C::NXF + C::NYF;
         const int fxl = ty * (TX + 1) + tx;
         const int fyl = C::NXF + ty * TX + tx;
@@ -992,18 +1003,31 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       }
 
       // ---- carry, window shift and shared-memory refill ----------------------
-      if constexpr (C::FAL) __syncthreads();
-      if constexpr (C::PSM && !C::TMA) __pipeline_wait_prior(0);
       if constexpr (C::TMA) {
-        // every thread waits for the boxes issued at the top of this plane
+        // the next plane's boxes: thread 0 waits and posts the outcome before
+        // the barrier that separates phase C from the refill (as above)
+        if (tid == 0) {
+          int f = 0;
+          if (more) f = mbar_wait(&s_mbar[1], ph_z) ? 0 : 1;
+          if (more_xy && !f) f = mbar_wait(&s_mbar[0], ph_p) ? 0 : 1;
+          s_fail_zp = f;
+        }
+        __syncthreads();
+        if (s_fail_zp) {
+          leave_after_timeout(tid, a.err, s_mbar, ph_p, ph_z, ph_q, more_xy, more, false);
+          return;
+        }
         if (more) {
-          fail |= !mbar_wait(&s_mbar[1], ph_z);
+          mbar_wait(&s_mbar[1], ph_z);
           ph_z ^= 1;
         }
         if (more_xy) {
-          fail |= !mbar_wait(&s_mbar[0], ph_p);
+          mbar_wait(&s_mbar[0], ph_p);
           ph_p ^= 1;
         }
+      } else {
+        if constexpr (C::FAL) __syncthreads();
+        if constexpr (C::PSM) __pipeline_wait_prior(0);
       }
       if (DIM == 3 && colt) {
 #pragma unroll
@@ -1052,24 +1076,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           }
         }
       }
-      if constexpr (C::TMA) {
-        // The plane's closing barrier also gathers the threads' wait results,
-        // so the whole CTA leaves together even when a copy lands so close to
-        // the deadline that only some threads saw it. Before leaving, thread 0
-        // (the issuer) waits, again bounded, for any copy still in flight, so
-        // none writes into the shared memory of an exited CTA.
-        if (__syncthreads_or(fail)) {
-          if (tid == 0) {
-            atomicExch(a.err, 1);
-            mbar_drain(&s_mbar[0], ph_p ^ 1u);
-            mbar_drain(&s_mbar[1], ph_z ^ 1u);
-            mbar_drain(&s_mbar[2], ph_q ^ 1u);
-          }
-          return;
-        }
-      } else {
-        __syncthreads();
-      }
+      __syncthreads();
     }
 
     if (a.last) cta_reduce_store<NT>(sS, s_red, a.partials + (int64_t)T.slot * kPartStride);

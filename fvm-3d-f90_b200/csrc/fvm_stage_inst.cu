@@ -4,7 +4,6 @@
 // be built with -fmad=false and the FP32 objects with fast single math).
 #include "fvm_aux.h"
 #include "fvm_stage.cuh"
-#include "fvm_step2d.cuh"
 
 #ifndef FVM_PREC
 #error "FVM_PREC not defined"
@@ -31,10 +30,6 @@ static bool fill(StageKernelInfo* out) {
   out->box_w = Cfg::TW;
   out->box_h = Cfg::PH;
   out->halo = Cfg::H;
-  if constexpr (DIM == 2)
-    out->step2d = reinterpret_cast<const void*>(&step2d_kernel<FVM_RECON, FLUX, FVM_PREC, TB, TX, TY, MINB>);
-  else
-    out->step2d = nullptr;
   return true;
 }
 

@@ -95,23 +95,6 @@ struct StageArgs {
   int32_t drop_copies;         // test of the timeout path: arm the barrier, skip the copy
 };
 
-// Arguments of the persistent 2D step kernel (fvm_step2d.cuh): the stage
-// arguments of every RK stage, the finalize's inputs and its grid barrier.
-struct Step2DArgs {
-  StageArgs st[4];          // stage m (1-based) in st[m - 1]
-  int32_t nstages;
-  int32_t nsteps;
-  const DevBlock* blocks;
-  const DevCase* cases;
-  const int* case_blk;
-  DevCaseState* state;
-  int32_t ncases;
-  int32_t ncounters;
-  int* counters;
-  unsigned int* bar;        // [0] arrivals, [1] generation; zero before the launch
-  int32_t* err;             // set to 2 when a barrier wait runs out
-};
-
 // Programmatic dependent launch. Inside the step graphs the kernels of a time
 // step are launched with programmatic stream serialization, so the CTAs of a
 // launch are scheduled while the one before it drains. Every kernel of that

@@ -29,8 +29,6 @@ def _lib():
         lib.fvm_profile_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int32), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
         lib.fvm_kernel_launches_per_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
-        lib.fvm_tune_set_fused_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
-        lib.fvm_fused_step_active.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
         lib._fvm_tuning_declared = True
     return lib
 
@@ -42,17 +40,6 @@ def set_tuning(solver, case_id: int, tile: int, zchunk: int) -> None:
 
 def set_tail_split(solver, case_id: int, split: int) -> None:
     solver._chk(_lib().fvm_tune_set_tail_split(solver.h, case_id, split))
-
-
-def set_fused_step(solver, mode: int) -> None:
-    """Persistent 2D step kernel: -1 / 1 where eligible (default), 0 never."""
-    solver._chk(_lib().fvm_tune_set_fused_step(solver.h, mode))
-
-
-def fused_step_active(solver) -> bool:
-    a = ctypes.c_int()
-    solver._chk(_lib().fvm_fused_step_active(solver.h, ctypes.byref(a)))
-    return bool(a.value)
 
 
 def time_step(solver, reps: int = 5) -> float:

@@ -249,22 +249,11 @@ int fvm_case_state(fvm_ctx* ctx, int case_id, double* t, double* dt, int64_t* st
 int fvm_tune_set(fvm_ctx* ctx, int case_id, int tile, int zchunk);
 int fvm_tune_set_tail_split(fvm_ctx* ctx, int case_id, int split);
 int fvm_tune_time_step(fvm_ctx* ctx, int reps, float* ms_per_step);
-/* Persistent 2D step kernel; no counterpart in the reference. A context
- * whose cases form one scheme group of 2D Euler blocks without connected
- * regions runs whole time steps in one cooperative launch (the RK stages
- * separated by grid barriers, the finalize inside) instead of one launch per
- * stage: the same arithmetic, bit-identical results, less launch latency on
- * small grids. mode -1 (default) or 1: use it where eligible; 0: never.
- * fvm_fused_step_active reports whether the current plan uses it. */
-int fvm_tune_set_fused_step(fvm_ctx* ctx, int mode);
-int fvm_fused_step_active(fvm_ctx* ctx, int* active);
 /* Profiling hooks; no counterpart in the reference. fvm_profile_step runs one
  * time step launch by launch with a CUDA event after each and returns the
  * device time of every launch (ms) and its kind (1 fused stage, 2 ghost
- * gather, 3 viscous, 4 finalize), always on the launch-per-stage path;
- * fvm_kernel_launches_per_step gives the number of kernels one
- * (graph-captured) time step launches, or 1 under the persistent 2D step
- * kernel (one launch per fvm_step call, whatever its step count). */
+ * gather, 3 viscous, 4 finalize); fvm_kernel_launches_per_step gives the
+ * number of kernels one (graph-captured) time step launches. */
 int fvm_profile_step(fvm_ctx* ctx, float* ms, int32_t* kinds, int cap, int* n);
 int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n);
 /* Test hook of the failure path; no counterpart in the reference. With on

@@ -161,53 +161,3 @@ def test_run_continues_from_the_current_step():
     assert why == abi.STOP_MAX_TIME and g.time()[2] == 5 + n
     o.step(5 + n)
     assert np.array_equal(g.get_state(0), o.get_state(0))
-
-
-@pytest.mark.parametrize("prec", [abi.PREC_FP64_EXACT, abi.PREC_FP64, abi.PREC_FP32_FLUX])
-@pytest.mark.parametrize("recon,flux,tile", [(abi.RECON_MUSCL, abi.FLUX_ROE, -1), (abi.RECON_WENO, abi.FLUX_AUSM, 3),
-                                             (abi.RECON_SIMPLE, abi.FLUX_VANLEER, 0)])
-def test_persistent_2d_step_equals_launch_per_stage(prec, recon, flux, tile):
-    # the persistent 2D step kernel (one cooperative launch per fvm_step call,
-    # grid barriers between the stages, finalize inside) against the
-    # launch-per-stage path: states, time and residuals bit-identical over
-    # single steps and runs of steps, CFL time step; the exact form also
-    # against the oracle
-    c = cases.riemann2d(n=70, seed=5, reconstruct=recon, flux_split=flux, limiter=abi.LIMITER_VANLEER,
-                        kappa=1.0 / 3.0, timestep_set=abi.DT_CFL, cfl=0.5, precision=prec)
-    runs = {}
-    for mode in (1, 0):
-        g = Solver(c.config())
-        c.apply(g, states=False)
-        tuning.set_fused_step(g, mode)
-        if tile >= 0:
-            tuning.set_tuning(g, 0, tile, 0)
-        g.set_state(0, c.states[0])
-        assert tuning.fused_step_active(g) == (mode == 1)
-        out = [g.step(1), g.step(7), g.step(1)]
-        runs[mode] = (out, g.get_state(0))
-        g.close()
-    (o1, q1), (o0, q0) = runs[1], runs[0]
-    assert np.array_equal(q1, q0)
-    for a, b in zip(o1, o0):
-        assert a[0] == b[0]
-        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2], equal_nan=True)
-    if prec == abi.PREC_FP64_EXACT:
-        o = c.apply(orc.Oracle(c.config()))
-        o.step(9)
-        assert np.array_equal(q1, o.get_state(0))
-
-
-def test_persistent_2d_step_only_where_eligible():
-    # periodic (connected) regions need the ghost gather: launch-per-stage path
-    c = cases.riemann2d(n=40, seed=2, dt=1e-3)
-    g = c.apply(Solver(c.config()))
-    assert tuning.fused_step_active(g)
-    g.close()
-    c.bcs = [(0, r, abi.BC_PERIODIC) for r in (1, 2, 3, 4)]
-    g = c.apply(Solver(c.config()))
-    assert not tuning.fused_step_active(g)
-    o = c.apply(orc.Oracle(c.config()))
-    g.step(3)
-    o.step(3)
-    assert np.array_equal(g.get_state(0), o.get_state(0))
-    g.close()
