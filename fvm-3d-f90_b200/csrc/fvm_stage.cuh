@@ -184,20 +184,19 @@ __device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
     if (global_ns() - t0 > 200000000ull) return;
   }
 }
-// Leaving the stage after a tensor copy timed out (the whole CTA, after a
-// barrier that published the outcome): thread 0 reports it and waits,
-// bounded, for every copy of this plane still in flight (the phases not yet
-// waited for: the operand boxes unless they already arrived, the z box if
-// issued, the plane box if issued), so none writes into the shared memory of
-// an exited CTA.
-__device__ __forceinline__ void leave_after_timeout(int tid, int32_t* err, uint64_t* mbar, uint32_t ph_p, uint32_t ph_z,
-                                                    uint32_t ph_q, bool plane_issued, bool z_issued,
-                                                    bool operands_pending) {
+// Leaving the stage after a tensor copy timed out (the whole CTA, after the
+// barrier at which it read the abort flag): thread 0 reports it and waits,
+// bounded, for the given phases of the three barriers, those of this plane's
+// copies; a phase that completed (or was never armed since the last
+// completed one) returns at once. So no copy writes into the shared memory
+// of an exited CTA.
+__device__ __forceinline__ void leave_after_timeout(int tid, int32_t* err, uint64_t* mbar, uint32_t par_p,
+                                                    uint32_t par_z, uint32_t par_q) {
   if (tid != 0) return;
   atomicExch(err, 1);
-  if (operands_pending) mbar_drain(&mbar[2], ph_q);
-  if (z_issued) mbar_drain(&mbar[1], ph_z);
-  if (plane_issued) mbar_drain(&mbar[0], ph_p);
+  mbar_drain(&mbar[2], par_q);
+  mbar_drain(&mbar[1], par_z);
+  mbar_drain(&mbar[0], par_p);
 }
 // 4D tiled tensor copy global -> this CTA's shared memory, completing on b.
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -359,7 +358,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
   __shared__ double s_red[6 * (NT / 32)];
   __shared__ int s_task;
   __shared__ __align__(8) uint64_t s_mbar[3];  // TMA: plane box, z box, RK operands
-  __shared__ int s_fail_q, s_fail_zp;            // TMA: thread 0's wait outcomes (1 = timed out)
+  __shared__ int s_abort;                        // TMA: a wait of this CTA ran out
   uint32_t ph_p = 0, ph_z = 0, ph_q = 0;       // TMA: expected phase parity of each mbarrier
 
   const int tid = threadIdx.x;
@@ -368,6 +367,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
   const int tx = tid % TX, ty = tid / TX;
   if constexpr (C::TMA) {
     if (tid == 0) {
+      s_abort = 0;
       mbar_init(&s_mbar[0], 1);
       mbar_init(&s_mbar[1], 1);
       mbar_init(&s_mbar[2], 1);
@@ -884,22 +884,16 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
         }
       }
-      // Tensor copies: thread 0 alone waits (bounded) for this plane's
-      // operand boxes and posts the outcome before the barrier, so the whole
-      // CTA takes the same decision after it without another barrier; the
-      // other threads then observe the completed phase themselves (at once).
-      if constexpr (C::TMA)
-        if (tid == 0 && do_xy) s_fail_q = mbar_wait(&s_mbar[2], ph_q) ? 0 : 1;
       __syncthreads();
 
       // ---- phase C: rhs, RK update, reductions -------------------------------
+      // Tensor copies: every thread waits (bounded) for the boxes issued at
+      // the top of this plane. A thread whose wait runs out raises the CTA's
+      // abort flag and carries on (its values are discarded); the whole CTA
+      // reads the flag after the plane's closing barrier and leaves together.
       if constexpr (C::TMA) {
         if (do_xy) {
-          if (s_fail_q) {
-            leave_after_timeout(tid, a.err, s_mbar, ph_p, ph_z, ph_q, more_xy, more, true);
-            return;
-          }
-          mbar_wait(&s_mbar[2], ph_q);
+          if (!mbar_wait(&s_mbar[2], ph_q)) s_abort = 1;
           ph_q ^= 1;
         }
       }
@@ -1003,31 +997,17 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       }
 
       // ---- carry, window shift and shared-memory refill ----------------------
+      if constexpr (C::FAL) __syncthreads();
+      if constexpr (C::PSM && !C::TMA) __pipeline_wait_prior(0);
       if constexpr (C::TMA) {
-        // the next plane's boxes: thread 0 waits and posts the outcome before
-        // the barrier that separates phase C from the refill (as above)
-        if (tid == 0) {
-          int f = 0;
-          if (more) f = mbar_wait(&s_mbar[1], ph_z) ? 0 : 1;
-          if (more_xy && !f) f = mbar_wait(&s_mbar[0], ph_p) ? 0 : 1;
-          s_fail_zp = f;
-        }
-        __syncthreads();
-        if (s_fail_zp) {
-          leave_after_timeout(tid, a.err, s_mbar, ph_p, ph_z, ph_q, more_xy, more, false);
-          return;
-        }
         if (more) {
-          mbar_wait(&s_mbar[1], ph_z);
+          if (!mbar_wait(&s_mbar[1], ph_z)) s_abort = 1;
           ph_z ^= 1;
         }
         if (more_xy) {
-          mbar_wait(&s_mbar[0], ph_p);
+          if (!mbar_wait(&s_mbar[0], ph_p)) s_abort = 1;
           ph_p ^= 1;
         }
-      } else {
-        if constexpr (C::FAL) __syncthreads();
-        if constexpr (C::PSM) __pipeline_wait_prior(0);
       }
       if (DIM == 3 && colt) {
 #pragma unroll
@@ -1077,6 +1057,16 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
         }
       }
       __syncthreads();
+      if constexpr (C::TMA) {
+        if (s_abort) {
+          // every thread read the flag after the same barrier: the CTA leaves
+          // together; thread 0 (the issuer) first waits, bounded, for the
+          // phases just waited for that may still have a copy in flight, so
+          // none writes into the shared memory of an exited CTA
+          leave_after_timeout(tid, a.err, s_mbar, ph_p ^ 1u, ph_z ^ 1u, ph_q ^ 1u);
+          return;
+        }
+      }
     }
 
     if (a.last) cta_reduce_store<NT>(sS, s_red, a.partials + (int64_t)T.slot * kPartStride);
