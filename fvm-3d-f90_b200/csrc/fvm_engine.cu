@@ -1129,7 +1129,6 @@ int Engine::plan() {
   CK(cudaStreamSynchronize(stream));
   planned_ = true;
   prepared_ = false;
-
   return build_graph();
 }
 
