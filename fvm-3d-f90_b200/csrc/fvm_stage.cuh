@@ -190,8 +190,9 @@ __device__ __forceinline__ void mbar_drain(uint64_t* b, uint32_t parity) {
 // copies; a phase that completed (or was never armed since the last
 // completed one) returns at once. So no copy writes into the shared memory
 // of an exited CTA.
-__device__ __forceinline__ void leave_after_timeout(int tid, int32_t* err, uint64_t* mbar, uint32_t par_p,
-                                                    uint32_t par_z, uint32_t par_q) {
+// (Not inlined: the error path stays out of the plane loop's code.)
+static __device__ __noinline__ void leave_after_timeout(int tid, int32_t* err, uint64_t* mbar, uint32_t par_p,
+                                                 uint32_t par_z, uint32_t par_q) {
   if (tid != 0) return;
   atomicExch(err, 1);
   mbar_drain(&mbar[2], par_q);
@@ -1058,7 +1059,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       }
       __syncthreads();
       if constexpr (C::TMA) {
-        if (s_abort) {
+        if (__builtin_expect(s_abort != 0, 0)) {
           // every thread read the flag after the same barrier: the CTA leaves
           // together; thread 0 (the issuer) first waits, bounded, for the
           // phases just waited for that may still have a copy in flight, so
