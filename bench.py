@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--tail-split", type=int, default=1, help="fixed tail split with --tile (1 = none)")
     ap.add_argument("--forms", default="fp64,fp32,exact",
                     help="comma list of precision forms, the first is the headline: fp64, fp32, exact")
-    ap.add_argument("--only", choices=["tgv", "riemann2d", "accuracy", "batched", "serve"], default=None,
+    ap.add_argument("--only", choices=["tgv", "riemann2d", "accuracy", "batched", "serve", "resid"], default=None,
                     help="run one secondary leg alone (its precision forms from --forms) and print its JSON")
     ap.add_argument("--accuracy-steps", type=int, default=1000, help="RK4 steps of the accuracy leg")
     return ap.parse_args()
@@ -629,16 +629,51 @@ def serve(args):
     def stream():
         return serving.poisson_stream(args.serve_requests, rate=rate, seed=7, make_case=make, steps=steps)
 
-    srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=1 << 21)
+    srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=None)
     out["continuous_batching"] = short(srv.run(stream()))
     srv.close()
-    srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=None)
-    out["continuous_batching_uncapped"] = short(srv.run(stream()))
+    srv = serving.Server(budget_cells=budget, chunk=8, max_active_cells=1 << 22)
+    out["continuous_batching_capped_4M_cells"] = short(srv.run(stream()))
     srv.close()
     out["one_at_a_time_fp64"] = short(serving.serve_one_at_a_time(stream(), precision=abi.PREC_FP64))
     out["arrival_rate_per_s"] = rate
     out["workload"] = (f"Riemann-2D / 8-block vortex (RK4) / NS TGV, edge {lo}..{hi} (2D: edge^1.5), "
                        f"{steps[0]}..{steps[1]} steps, FP32 flux; budget {budget * 160 / 1e9:.0f} GB")
+    return out
+
+
+# ---------------------------------------------------------------- residual norms leg
+def resid_leg(args):
+    """fvm_residual_norms and fvm_residual_norms_noalloc on one n^3 block's
+    rhs already in device memory (the ClassIteration%compute_residual_sub
+    step of a host that keeps rhs on the device): time per call, including
+    the per-call scratch allocation of the first and the stream sync of both,
+    and the rhs bytes read per second."""
+    import ctypes
+
+    import torch
+
+    from fvm3d import abi
+
+    lib = abi.load_library()
+    lib.fvm_residual_norms_noalloc.argtypes = lib.fvm_residual_norms.argtypes
+    n = args.n
+    rhs = torch.randn(5 * n * n * n, dtype=torch.float64, device="cuda")
+    res = torch.zeros(6, dtype=torch.float64, device="cuda")
+    nv = (ctypes.c_int64 * 3)(n, n, n)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {"cells": n ** 3, "unit": "GB/s"}
+    for name in ("fvm_residual_norms", "fvm_residual_norms_noalloc"):
+        fn = getattr(lib, name)
+        for _ in range(3):
+            assert fn(ctypes.c_void_p(rhs.data_ptr()), nv, ctypes.c_void_p(res.data_ptr()), st) == 0
+        torch.cuda.synchronize()
+        reps = 20
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn(ctypes.c_void_p(rhs.data_ptr()), nv, ctypes.c_void_p(res.data_ptr()), st)
+        sec = (time.perf_counter() - t0) / reps
+        out[name] = {"us_per_call": sig(sec * 1e6), "rhs_read_gbs": sig(40.0 * n ** 3 / sec / 1e9)}
     return out
 
 
@@ -688,7 +723,7 @@ def main():
 
     if args.only:
         leg = {"tgv": tgv, "riemann2d": riemann2d_leg, "accuracy": accuracy_leg, "batched": batched,
-               "serve": serve}[args.only]
+               "serve": serve, "resid": resid_leg}[args.only]
         if dist.rank == 0:
             print(json.dumps({"leg": args.only, **leg(args)}))
         dist.close()
@@ -701,6 +736,26 @@ def main():
                  "clocks": res.pop("clocks")})
     if "e2e" in res:
         line["e2e"] = res.pop("e2e")
+    line["timing"] = res.pop("timing")
+    ratios = {}
+    if "vortex_fp32_over_fp64" in res:
+        ratios["vortex"] = res.pop("vortex_fp32_over_fp64")
+    # the GPU legs first, the CPU baseline last: the oracle's OpenMP threads
+    # keep spinning for a while after it returns and would slow the host
+    # loops of the serving leg
+    legs = {}
+    if dist.world == 1 and not args.no_serve:
+        legs["serving"] = serve(args)
+    if dist.world == 1 and not args.no_batch:
+        b = batched(args)
+        legs["batched"] = b
+        ratios["batch"] = b["fp32_over_fp64"]
+        t = tgv(args)
+        legs["navier_stokes_tgv"] = t
+        ratios["tgv"] = t.get("fp32_over_fp64")
+        r2 = riemann2d_leg(args)
+        legs["riemann2d_256"] = r2
+        ratios["riemann2d"] = r2.get("fp32_over_fp64")
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu:
         v, th, sec = cpu_oracle(args.n, 30, 1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": th, "kind": "port",
@@ -709,25 +764,11 @@ def main():
         # the reference itself is serial: the same restatement on one thread
         v1, _, sec1 = cpu_oracle(args.n, 3, 0, threads=1)
         line["cpu_baseline_1thread"] = {"value": sig(v1), "cores": 1, "sample": f"3 RK4 steps ({sec1:.1f} s)"}
-    line["timing"] = res.pop("timing")
-    ratios = {}
-    if "vortex_fp32_over_fp64" in res:
-        ratios["vortex"] = res.pop("vortex_fp32_over_fp64")
-    if dist.world == 1 and not args.no_serve:
-        sv = serve(args)
-        line["serving"] = sv
-        line["p50_s"] = sv["continuous_batching"]["p50_s"]
-        line["p99_s"] = sv["continuous_batching"]["p99_s"]
-    if dist.world == 1 and not args.no_batch:
-        b = batched(args)
-        line["batched"] = b
-        ratios["batch"] = b["fp32_over_fp64"]
-        t = tgv(args)
-        line["navier_stokes_tgv"] = t
-        ratios["tgv"] = t.get("fp32_over_fp64")
-        r2 = riemann2d_leg(args)
-        line["riemann2d_256"] = r2
-        ratios["riemann2d"] = r2.get("fp32_over_fp64")
+    if "serving" in legs:
+        line["serving"] = legs.pop("serving")
+        line["p50_s"] = line["serving"]["continuous_batching"]["p50_s"]
+        line["p99_s"] = line["serving"]["continuous_batching"]["p99_s"]
+    line.update(legs)
     # the precision forms beside the headline, and the FP32 / FP64 speed
     # ratio of every configuration, last (the end of the line is what a
     # truncated log keeps)

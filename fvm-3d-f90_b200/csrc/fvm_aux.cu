@@ -30,15 +30,28 @@ namespace fvm {
 constexpr int kGatherPer = 4;
 __global__ void __launch_bounds__(256, 4) gather_kernel(double* __restrict__ base, int64_t vs, const int2* __restrict__ pairs,
                               int64_t npairs) {
-  pdl_wait();
-  pdl_trigger();
   const int64_t G = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += G * kGatherPer) {
-    int2 p[kGatherPer];
+  // the pairs change only when the engine re-plans between steps: the first
+  // round's are loaded before the wait for the stage kernel that wrote the
+  // values, so their round trip overlaps its tail
+  int2 p[kGatherPer];
+  {
+    const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
 #pragma unroll
     for (int j = 0; j < kGatherPer; ++j) {
       const int64_t i = i0 + j * G;
       p[j] = i < npairs ? pairs[i] : make_int2(-1, -1);
+    }
+  }
+  pdl_wait();
+  pdl_trigger();
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < npairs; i0 += G * kGatherPer) {
+    if (i0 != blockIdx.x * (int64_t)blockDim.x + threadIdx.x) {
+#pragma unroll
+      for (int j = 0; j < kGatherPer; ++j) {
+        const int64_t i = i0 + j * G;
+        p[j] = i < npairs ? pairs[i] : make_int2(-1, -1);
+      }
     }
     double val[kGatherPer][5];
 #pragma unroll
@@ -138,9 +151,10 @@ __global__ void init_dt_kernel(const DevCase* cases, DevCaseState* st, const uns
 // fvm_finalize.cuh).
 __global__ void finalize_kernel(const DevBlock* blocks, const DevCase* cases, const int* case_blk, DevCaseState* st,
                                 const double* partials, int* counters, int ncounters) {
-  pdl_wait();
-  pdl_trigger();
-  finalize_case(blockIdx.x, blocks, cases, case_blk, st, partials, counters, ncounters);
+  finalize_case(blockIdx.x, blocks, cases, case_blk, st, partials, counters, ncounters, [] {
+    pdl_wait();
+    pdl_trigger();
+  });
 }
 
 // ---------------------------------------------------------------- launchers

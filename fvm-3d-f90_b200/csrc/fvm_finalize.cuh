@@ -19,37 +19,62 @@ namespace fvm {
 // root of latency. Any multiple of 32 threads gives the same sums (each
 // block's reduction and the fold order do not depend on the warp count). The
 // CTA of case 0 also zeroes the stage work-queue counters for the next step.
+// The descriptors (case, block list, block sizes and task ranges) change only
+// when the engine re-plans between steps, so they are read before `wait`
+// (the programmatic-launch wait for the step's last kernel) and their memory
+// round trips overlap that kernel's tail; partials, counters and the case
+// state are touched only after it.
+template <class Wait>
 __device__ __forceinline__ void finalize_case(int c, const DevBlock* blocks, const DevCase* cases, const int* case_blk,
                                               DevCaseState* st, const double* partials, int* counters,
-                                              int ncounters) {
+                                              int ncounters, Wait wait) {
   constexpr int kMaxW = 8;
   __shared__ double red[kMaxW][6];
   __shared__ double redm[kMaxW];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int NW = min(kMaxW, (int)(blockDim.x >> 5));
   const DevCase& C = cases[c];
+  const int nblocks = C.nblocks, block0 = C.block0, ts_set = C.timestep_set;
+  const double dt_fixed = C.dt_fixed, cfl = C.cfl;
+  // the first block of this warp
+  int pf_task0 = 0, pf_ntask = 0;
+  double pf_npt = 1.0;
+  if (warp < NW && warp < nblocks) {
+    const DevBlock& B = blocks[case_blk[block0 + warp]];
+    pf_task0 = B.task0;
+    pf_ntask = B.ntask;
+    pf_npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
+  }
+  wait();
   if (c == 0)
     for (int i = tid; i < ncounters; i += blockDim.x) counters[i] = 0;
-  if (C.nblocks == 0) return;  // removed case (uniform over the CTA)
+  if (nblocks == 0) return;  // removed case (uniform over the CTA)
   double res[6] = {0, 0, 0, 0, 0, 0};
   double wmax = 0.0;
-  for (int b0 = 0; b0 < C.nblocks; b0 += NW) {
+  for (int b0 = 0; b0 < nblocks; b0 += NW) {
     const int bb = b0 + warp;
-    if (warp < NW && bb < C.nblocks) {
-      const DevBlock& B = blocks[case_blk[C.block0 + bb]];
+    if (warp < NW && bb < nblocks) {
+      int task0 = pf_task0, ntask = pf_ntask;
+      double npt = pf_npt;
+      if (b0 > 0) {
+        const DevBlock& B = blocks[case_blk[block0 + bb]];
+        task0 = B.task0;
+        ntask = B.ntask;
+        npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
+      }
       // each lane loads kU partials before adding them (in a fixed order), so
       // a block of many tasks costs one memory round trip per 32 * kU tasks
       constexpr int kU = 8;
       double s[5] = {0, 0, 0, 0, 0}, m = 0.0;
-      for (int t = lane; t < B.ntask; t += 32 * kU) {
+      for (int t = lane; t < ntask; t += 32 * kU) {
         double q[kU][6];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
           const int tt = t + 32 * u;
-          if (tt < B.ntask) {
-            const double* p = partials + (int64_t)(B.task0 + tt) * kPartStride;
+          if (tt < ntask) {
+            const double* p = partials + (int64_t)(task0 + tt) * kPartStride;
 #pragma unroll
-            for (int v = 0; v < 6; ++v) q[u][v] = __ldcg(p + v);  // written by other CTAs (maybe this launch)
+            for (int v = 0; v < 6; ++v) q[u][v] = p[v];
           } else {
 #pragma unroll
             for (int v = 0; v < 6; ++v) q[u][v] = 0.0;  // adds nothing: same sums as task by task
@@ -69,7 +94,6 @@ __device__ __forceinline__ void finalize_case(int c, const DevBlock* blocks, con
         m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
       }
       if (lane == 0) {
-        const double npt = (double)((int64_t)B.n[0] * B.n[1] * B.n[2]);
         double res2_t = 0.0;
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -83,7 +107,7 @@ __device__ __forceinline__ void finalize_case(int c, const DevBlock* blocks, con
     }
     __syncthreads();
     if (tid == 0) {
-      for (int w = 0; w < NW && b0 + w < C.nblocks; ++w) {
+      for (int w = 0; w < NW && b0 + w < nblocks; ++w) {
 #pragma unroll
         for (int v = 0; v < 6; ++v) res[v] = __dsqrt_rn(__dadd_rn(__dmul_rn(res[v], res[v]), red[w][v]));
         wmax = fmax(wmax, redm[w]);
@@ -104,7 +128,7 @@ __device__ __forceinline__ void finalize_case(int c, const DevBlock* blocks, con
       S.status = 4;  // FVM_ERR_NONFINITE
     else if (res[5] > 1.0E10)
       S.status = 5;  // FVM_ERR_DIVERGED
-    S.dt = (C.timestep_set == 0) ? C.dt_fixed : __ddiv_rn(C.cfl, wmax);
+    S.dt = (ts_set == 0) ? dt_fixed : __ddiv_rn(cfl, wmax);
   }
 }
 
