@@ -199,8 +199,20 @@ int Engine::add_case(const fvm_config& c, int* case_id) {
     return fail(FVM_ERR_INVALID, "the arena was laid out for 3 RK stages");
   HCase hc;
   hc.cfg = c;
-  cases.push_back(hc);
-  if (case_id) *case_id = (int)cases.size() - 1;
+  // a removed case's slot is taken again (never slot 0, the context's own
+  // first case, whose removal fvm_step reports as "no outputs"), so a
+  // long-running server's case list, device state array and finalize grid
+  // stay the size of its running set
+  int slot = -1;
+  for (size_t i = 1; i < cases.size() && slot < 0; ++i)
+    if (cases[i].dead) slot = (int)i;
+  if (slot < 0) {
+    cases.push_back(hc);
+    slot = (int)cases.size() - 1;
+  } else {
+    cases[slot] = hc;
+  }
+  if (case_id) *case_id = slot;
   invalidate();
   return FVM_OK;
 }
@@ -244,9 +256,18 @@ int Engine::add_block(int case_id, const int64_t n[3], const double dr[3], int* 
     b.n[d] = n[d];
     b.dr[d] = dr[d];
   }
-  blocks.push_back(b);
-  cases[case_id].blocks.push_back((int)blocks.size() - 1);
-  if (blk) *blk = (int)blocks.size() - 1;
+  // a removed block's slot is taken again (its arena range was freed)
+  int slot = -1;
+  for (size_t i = 0; i < blocks.size() && slot < 0; ++i)
+    if (blocks[i].dead) slot = (int)i;
+  if (slot < 0) {
+    blocks.push_back(b);
+    slot = (int)blocks.size() - 1;
+  } else {
+    blocks[slot] = b;
+  }
+  cases[case_id].blocks.push_back(slot);
+  if (blk) *blk = slot;
   invalidate();
   return FVM_OK;
 }

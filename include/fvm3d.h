@@ -228,7 +228,9 @@ int fvm_block_cells(int idimension, const int64_t nvert[3], int64_t* cells);
 int fvm_add_case(fvm_ctx* ctx, const fvm_config* cfg, int* case_id);
 /* fvm_add_block for a given case; block ids are unique across cases. */
 int fvm_add_case_block(fvm_ctx* ctx, int case_id, const int64_t nvert[3], const double dr[3], int* blk);
-/* Remove a case and free its arena ranges. */
+/* Remove a case and free its arena ranges. Later additions reuse the ids of
+ * removed cases (except case 0, the context's own first case) and of their
+ * blocks, so a long-running engine's tables stay the size of its live set. */
 int fvm_remove_case(fvm_ctx* ctx, int case_id);
 /* Time, last dt, step count, residuals and status (FVM_OK, FVM_ERR_NONFINITE,
  * FVM_ERR_DIVERGED) of one case. Any pointer may be NULL. */
