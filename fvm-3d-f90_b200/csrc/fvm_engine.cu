@@ -673,7 +673,13 @@ static cudaError_t grow_buf(T** p, size_t* cap, size_t n) {
 }
 
 int Engine::plan() {
-  destroy_graphs();
+  // the instantiated step graphs are kept: build_graph() updates them in
+  // place when the new step has the same shape (no launch can use them
+  // before the plan completes: planned_ stays false until then)
+  if (graph_) cudaGraphDestroy(graph_);
+  if (graphm_) cudaGraphDestroy(graphm_);
+  graph_ = nullptr;
+  graphm_ = nullptr;
   if (!laid_out_) {
     int rc = layout();
     if (rc) return rc;
@@ -1271,8 +1277,12 @@ cudaError_t Engine::launch_steps(int nsteps) {
   return cudaSuccess;
 }
 
+// Capture one time step (and kMultiSteps of them) and make them launchable:
+// an instantiated graph of an earlier plan is updated in place when the new
+// capture has its shape (same kernels and dependencies: a serving engine
+// admitting or retiring cases of the same schemes), which costs a fraction of
+// a new instantiation; otherwise it is instantiated again.
 int Engine::build_graph() {
-  destroy_graphs();
   while (side_.size() < groups.size()) {
     cudaStream_t st;
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -1284,33 +1294,39 @@ int Engine::build_graph() {
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     fork_ev_.push_back(e);
   }
-  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  auto capture = [&](int nsteps, int* launches, cudaGraph_t* out) -> int {
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    for (int i = 0; i < nsteps && rc == 0; ++i) rc = enqueue_step(nullptr, 0, nullptr, i == 0 ? launches : nullptr);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    *out = g;
+    return FVM_OK;
+  };
+  auto make_exec = [&](cudaGraph_t g, cudaGraphExec_t* exec) -> int {
+    if (*exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(*exec, g, &info) == cudaSuccess) return FVM_OK;
+      (void)cudaGetLastError();  // a different shape: instantiate anew
+      cudaGraphExecDestroy(*exec);
+      *exec = nullptr;
+    }
+    CK(cudaGraphInstantiate(exec, g, 0));
+    return FVM_OK;
+  };
   int launches = 0;
-  int rc = enqueue_step(nullptr, 0, nullptr, &launches);
-  cudaGraph_t g = nullptr;
-  cudaError_t e2 = cudaStreamEndCapture(stream, &g);
-  if (rc) {
-    if (g) cudaGraphDestroy(g);
-    return rc;
-  }
-  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
-  graph_ = g;
-  CK(cudaGraphInstantiate(&gexec_, graph_, 0));
+  int rc = capture(1, &launches, &graph_);
+  if (!rc) rc = make_exec(graph_, &gexec_);
+  if (rc) return rc;
   kernel_launches_per_step = launches;
-  // the same step kMultiSteps times in one graph
-  CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-  rc = 0;
-  for (int i = 0; i < kMultiSteps && rc == 0; ++i) rc = enqueue_step(nullptr, 0, nullptr, nullptr);
-  g = nullptr;
-  e2 = cudaStreamEndCapture(stream, &g);
-  if (rc) {
-    if (g) cudaGraphDestroy(g);
-    return rc;
-  }
-  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
-  graphm_ = g;
-  CK(cudaGraphInstantiate(&gexecm_, graphm_, 0));
-  return FVM_OK;
+  rc = capture(kMultiSteps, nullptr, &graphm_);
+  if (!rc) rc = make_exec(graphm_, &gexecm_);
+  return rc;
 }
 
 int Engine::profile_step(float* ms, int* kinds, int cap, int* n) {
