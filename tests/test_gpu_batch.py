@@ -215,3 +215,22 @@ def test_running_case_unchanged_when_another_joins():
         for k, g in enumerate(ids):
             assert np.array_equal(s.get_state(g), ref[k]), (prec, k)
         s.close()
+
+
+def test_server_failing_request_does_not_disturb_the_others():
+    # a request whose residual goes NaN (the reference WENO5 + AUSM on a
+    # strong blast) ends FAILED with FVM_ERR_NONFINITE while the requests
+    # served beside it finish and equal their runs alone
+    bad = cases.blast((20, 20, 20), seed=0, reconstruct=abi.RECON_WENO, flux_split=abi.FLUX_AUSM)
+    good = [cases.taylor_green(N=16), cases.riemann2d(n=40, seed=2, dt=1e-3)]
+    srv = serving.Server(budget_cells=1 << 22, chunk=2)
+    ids = [srv.submit(c, 6) for c in [good[0], bad, good[1]]]
+    states = [srv.wait(i) for i in ids]
+    assert states == [abi.REQ_DONE, abi.REQ_FAILED, abi.REQ_DONE], states
+    assert srv.poll(ids[1])["status"] == 4
+    for i, c in ((ids[0], good[0]), (ids[2], good[1])):
+        got = srv.fetch(i, c)
+        ref = alone(c, 6)
+        for g, r in zip(got, ref):
+            assert np.array_equal(g, r)
+    srv.close()
