@@ -21,6 +21,15 @@ Cases:
   * tgv12: the Navier-Stokes Taylor-Green vortex on 12^3 cells, MUSCL /
     Van Albada + Roe, central viscous fluxes, SSP-RK3, CFL 0.5; 8 steps, with
     kinetic-energy and enstrophy histories.
+
+One fixture comes from the reference itself rather than the oracle:
+  * riemann2d_reference_devlog.json: what the reference's own run of
+    case/Riemann-2D.nml logged in case/dev.log (written by global_devlog from
+    class_flow_field.f90:321 and class_time_discret.f90:177,187): the flow
+    time after each step as printed (17 significant digits, so each string
+    names one double), and the trace lines counted per step (RK stages,
+    directions, reconstruction and flux-split names, blocks). It is written
+    only when the reference tree is present.
 """
 from __future__ import annotations
 
@@ -40,6 +49,7 @@ from fvm3d import cases  # noqa: E402
 from fvm3d.namelist import parse_case  # noqa: E402
 
 REFERENCE_CASE = "/root/reference/case/Riemann-2D.nml"
+REFERENCE_DEVLOG = "/root/reference/case/dev.log"
 
 # name -> (case builder, steps)
 FIXTURES = {
@@ -80,7 +90,40 @@ def run(case, steps, target):
     return out
 
 
+def devlog_fixture(path):
+    """The reference run's log as a fixture: printed flow times, in step
+    order, and the per-step structure of its trace lines."""
+    with open(path) as f:
+        lines = [ln.strip() for ln in f.read().splitlines()]
+    times = [ln.split("Flowfield real time", 1)[1].strip() for ln in lines if "Flowfield real time" in ln]
+    steps = [int(ln.split("Print residual step", 1)[1]) for ln in lines if "Print residual step" in ln]
+    assert steps == list(range(len(times))), "one time line per printed step"
+    # the trace of one complete step (step 0, up to the next step's header)
+    first = lines.index("-- Print residual step 0")
+    nxt = lines.index("-- Print residual step 1")
+    step0 = [ln for ln in lines[first:nxt] if ln != "--"]
+    return {
+        "source": "case/dev.log of the reference (its own run of case/Riemann-2D.nml)",
+        "dt_namelist": "2.0E-4",
+        "printed_time": times,
+        "time": [float(t) for t in times],
+        "rk_stages_per_step": sum(1 for ln in step0 if ln.startswith("-- RK stage")),
+        "directions_per_stage": sorted({int(ln.split(":")[1]) for ln in step0 if ln.startswith("-- Direction:")}),
+        "reconstruction": sorted({ln.split("(")[1].rstrip(")") for ln in step0 if ln.startswith("-- Reconstruction")}),
+        "flux_split": sorted({ln.split("(")[1].rstrip(")") for ln in step0 if ln.startswith("-- Flux split")}),
+        "blocks": sorted({ln.rsplit(" ", 1)[1] for ln in step0 if ln.startswith("-- Time Stepping")}),
+        "residual_computed_per_step": sum(1 for ln in step0 if ln == "-- Compute residual"),
+    }
+
+
 def main():
+    if os.path.exists(REFERENCE_DEVLOG):
+        fx = devlog_fixture(REFERENCE_DEVLOG)
+        path = os.path.join(HERE, "riemann2d_reference_devlog.json")
+        with open(path, "w") as f:
+            json.dump(fx, f, indent=1)
+            f.write("\n")
+        print(f"{path}: {len(fx['time'])} printed flow times")
     if os.path.exists(REFERENCE_CASE):
         with open(REFERENCE_CASE) as f:
             spec = parse_case(f.read())

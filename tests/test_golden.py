@@ -1,7 +1,14 @@
 """Golden fixtures (tests/golden/*.npz, written by tests/golden/make_golden.py
 from the oracle): the oracle itself (CPU) and the GPU path's exact FP64 form
 (through the C ABI) must reproduce each fixture's per-step time and residual
-history, final state and last-stage rhs bit for bit."""
+history, final state and last-stage rhs bit for bit.
+
+tests/golden/riemann2d_reference_devlog.json holds what the reference's own
+run of case/Riemann-2D.nml logged (its case/dev.log): the flow time after each
+of 269 steps, printed to 17 significant digits, and the per-step structure of
+the trace. The oracle and every GPU precision form must reach the same
+doubles, and the configuration the tests rebuild for that case file must take
+the steps the run took."""
 import json
 import os
 
@@ -84,4 +91,55 @@ def test_gpu_exact_reproduces_golden(name):
     g = case.apply(Solver(case.config(store_rhs=1)))
     # the GPU sums residual norms in a different (deterministic) order
     replay(case, steps, g, res_exact=False)
+    g.close()
+
+
+def load_devlog():
+    with open(os.path.join(HERE, "riemann2d_reference_devlog.json")) as f:
+        return json.load(f)
+
+
+def test_devlog_fixture_is_self_consistent():
+    fx = load_devlog()
+    # 17 significant digits: each printed string names exactly the double stored beside it
+    assert [float(s) for s in fx["printed_time"]] == fx["time"]
+    assert len(fx["time"]) == 269
+    assert all(b > a for a, b in zip(fx["time"], fx["time"][1:]))
+
+
+def test_reference_case_takes_the_steps_its_run_logged():
+    # class_time_discret.f90:177,187 log each RK stage and block; class_space_discret.f90:132-173
+    # each direction with its reconstruction and flux-split names
+    fx = load_devlog()
+    case = cases.riemann2d_reference()
+    cfg = case.config()
+    assert cfg.rk_stages == fx["rk_stages_per_step"] == 3
+    assert cfg.idimension == len(fx["directions_per_stage"]) == 2
+    assert fx["reconstruction"] == ["MUSCL"] and cfg.reconstruct == abi.RECON_MUSCL
+    assert fx["flux_split"] == ["Roe"] and cfg.flux_split == abi.FLUX_ROE
+    assert len(case.blocks) == len(fx["blocks"]) == 1
+    assert fx["residual_computed_per_step"] == 1
+    assert cfg.timestep_set == abi.DT_FIXED and cfg.dt == float(fx["dt_namelist"])
+
+
+def test_oracle_time_history_matches_reference_run():
+    # ClassTimeDiscret%solve: time = time + dt, then set_realtime logs it (class_time_discret.f90:142-144)
+    fx = load_devlog()
+    case = cases.riemann2d_reference()
+    o = case.apply(orc.Oracle(case.config()))
+    for s, want in enumerate(fx["time"]):
+        t = o.step(1)[0]
+        assert t == want, f"step {s}: {t!r} != {fx['printed_time'][s]}"
+    o.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [abi.PREC_FP64_EXACT, abi.PREC_FP64, abi.PREC_FP32_FLUX])
+def test_gpu_time_history_matches_reference_run(prec):
+    fx = load_devlog()
+    case = cases.riemann2d_reference()
+    g = case.apply(Solver(case.config(precision=prec)))
+    for s, want in enumerate(fx["time"]):
+        t = g.step(1)[0]
+        assert t == want, f"step {s}: {t!r} != {fx['printed_time'][s]}"
     g.close()
