@@ -103,7 +103,7 @@ void Engine::release() {
   }
   for (auto& r : role_) r = nullptr;
   void* ptrs[] = {visc_,     d_blocks_,   d_cases_,     d_case_blk_, d_state_, d_tasks_,
-                  d_partials_, d_pairs_, d_counters_, d_casemax_,  d_staging_};
+                  d_partials_, d_pairs_, d_pairs_alt_, d_counters_, d_casemax_,  d_staging_};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   visc_ = nullptr;
@@ -115,6 +115,8 @@ void Engine::release() {
   d_tasks_ = nullptr;
   d_partials_ = nullptr;
   d_pairs_ = nullptr;
+  d_pairs_alt_ = nullptr;
+  cap_pairs_alt_ = 0;
   d_counters_ = nullptr;
   d_casemax_ = nullptr;
   cap_blocks_ = cap_cases_ = cap_case_blk_ = cap_tasks_ = cap_partials_ = cap_pairs_ = cap_counters_ = cap_casemax_ = 0;
@@ -126,6 +128,7 @@ void Engine::release() {
   for (auto p : d_tmap_)
     if (p) cudaFree(p);
   d_tmap_.clear();
+  cap_tmap_.clear();
   if (d_err_) cudaFree(d_err_);
   d_err_ = nullptr;
   if (d_dtmask_) cudaFree(d_dtmask_);
@@ -739,9 +742,14 @@ int Engine::plan() {
     hc.group = gi;
   }
   for (auto& G : groups) {
-    CK(cudaFuncSetAttribute(G.k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.k.smem));
-    int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, G.k.fn, G.k.threads, G.k.smem));
+    int occ = -1;
+    for (const auto& e : occ_cache_)
+      if (e.first == G.k.fn) occ = e.second;
+    if (occ < 0) {
+      CK(cudaFuncSetAttribute(G.k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.k.smem));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, G.k.fn, G.k.threads, G.k.smem));
+      occ_cache_.emplace_back(G.k.fn, occ);
+    }
     if (occ < 1) return fail(FVM_ERR_UNSUPPORTED, "stage kernel does not fit on an SM");
     G.grid = occ * num_sms;
   }
@@ -947,19 +955,85 @@ int Engine::plan() {
   //    on its own blocks (connections never cross cases) and their arena
   //    offsets, which never change while the case lives, so they are built
   //    once per case and reused by every later re-plan (the serving loop
-  //    re-plans at each admission and retirement).
-  std::vector<int64_t> pairs;
-  std::vector<int64_t> cp;  // pairs of the case being built
+  //    re-plans at each admission and retirement). Cell offsets within a role
+  //    slab stay below 2^31 (a slab of 2^31 cells would take 344 GB in the 4
+  //    roles, twice the HBM): 8 bytes per pair.
+  if (cap_ >= ((int64_t)1 << 31)) return fail(FVM_ERR_INVALID, "arena too large for 32-bit ghost offsets");
+  std::vector<int32_t> cp;  // pairs of the case being built
   auto add_pair = [&](int bi, const int64_t x[3]) -> int {
     int64_t y[3] = {x[0], x[1], x[2]};
     int src_blk = -1;
     if (resolve(bi, y, &src_blk) != 0) return -1;
     const HBlock& b = blocks[bi];
     const HBlock& s = blocks[src_blk];
-    cp.push_back(b.slab_off + b.org + x[0] + x[1] * b.sy + x[2] * b.sz);
-    cp.push_back(s.slab_off + s.org + y[0] + y[1] * s.sy + y[2] * s.sz);
+    cp.push_back((int32_t)(b.slab_off + b.org + x[0] + x[1] * b.sy + x[2] * b.sz));
+    cp.push_back((int32_t)(s.slab_off + s.org + y[0] + y[1] * s.sy + y[2] * s.sz));
     return 0;
   };
+  // One connection's ghost cells. When the connection's range lies wholly
+  // outside the block along one axis and wholly inside along the others, in
+  // a region that is not transmissive, no earlier connection of the block
+  // overlaps it, and its image under the donor map is all real donor cells,
+  // resolve() would take exactly one hop through this connection for every
+  // cell: the pairs are then the affine map itself, row by row.
+  auto add_conn = [&](int bi, size_t ci) -> int {
+    const HBlock& b = blocks[bi];
+    const HConn& c = b.conns[ci];
+    int out = 0, inside = 0, region = 0;
+    for (int d = 0; d < 3; ++d) {
+      if (c.range[d][1] < 0) {
+        ++out;
+        region = 2 * d + 1;
+      } else if (c.range[d][0] >= b.n[d]) {
+        ++out;
+        region = 2 * d + 2;
+      } else if (c.range[d][0] >= 0 && c.range[d][1] < b.n[d]) {
+        ++inside;
+      }
+    }
+    bool direct = out == 1 && inside == 2 && b.bc[region - 1] != FVM_BC_TRANSMISSIVE;
+    for (size_t e = 0; e < ci && direct; ++e) {
+      const HConn& o = b.conns[e];
+      bool ov = true;
+      for (int d = 0; d < 3; ++d) ov = ov && o.range[d][0] <= c.range[d][1] && c.range[d][0] <= o.range[d][1];
+      direct = !ov;
+    }
+    const HBlock& s = blocks[c.donor];
+    int64_t ys[3] = {0, 0, 0};  // donor offset step per unit step of x along each axis
+    int64_t y0[3];
+    const int64_t sst[3] = {1, s.sy, s.sz};
+    for (int d = 0; d < 3 && direct; ++d) {
+      const int dd = std::abs(c.dtype[d]) - 1;
+      const int64_t sg = c.dtype[d] > 0 ? 1 : -1;
+      const int64_t a0 = c.drange[d][0], a1 = c.drange[d][0] + sg * (c.range[d][1] - c.range[d][0]);
+      direct = std::min(a0, a1) >= 0 && std::max(a0, a1) < s.n[dd];
+      y0[dd] = a0;
+      ys[d] = sg * sst[dd];
+    }
+    if (direct) {
+      const int64_t src0 = s.slab_off + s.org + y0[0] + y0[1] * s.sy + y0[2] * s.sz;
+      const int64_t dst0 = b.slab_off + b.org;
+      const int64_t ni = c.range[0][1] - c.range[0][0] + 1;
+      for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
+        for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j) {
+          int64_t dst = dst0 + c.range[0][0] + j * b.sy + k * b.sz;
+          int64_t src = src0 + (j - c.range[1][0]) * ys[1] + (k - c.range[2][0]) * ys[2];
+          for (int64_t i = 0; i < ni; ++i, ++dst, src += ys[0]) {
+            cp.push_back((int32_t)dst);
+            cp.push_back((int32_t)src);
+          }
+        }
+      return 0;
+    }
+    for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
+      for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j)
+        for (int64_t i = c.range[0][0]; i <= c.range[0][1]; ++i) {
+          const int64_t x[3] = {i, j, k};
+          if (add_pair(bi, x) != 0) return -1;
+        }
+    return 0;
+  };
+  int64_t npairs_total = 0;
   for (int ci : live_cases) {
     HCase& hc = cases[ci];
     std::vector<int64_t> key;
@@ -968,13 +1042,8 @@ int Engine::plan() {
       cp.clear();
       for (int bi : hc.blocks) {
         const HBlock& b = blocks[bi];
-        for (const auto& c : b.conns)
-          for (int64_t k = c.range[2][0]; k <= c.range[2][1]; ++k)
-            for (int64_t j = c.range[1][0]; j <= c.range[1][1]; ++j)
-              for (int64_t i = c.range[0][0]; i <= c.range[0][1]; ++i) {
-                const int64_t x[3] = {i, j, k};
-                if (add_pair(bi, x) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
-              }
+        for (size_t c = 0; c < b.conns.size(); ++c)
+          if (add_conn(bi, c) != 0) return fail(FVM_ERR_INVALID, "ghost cell without a real donor");
         if (hc.cfg.equation == FVM_EQ_NAVIER_STOKES) {
           // layer-1 edge ghosts read by the viscous stencil where both regions
           // are connected (a transmissive axis is clamped on load instead)
@@ -999,10 +1068,11 @@ int Engine::plan() {
       hc.pairs_cache = cp;
       hc.pairs_key = key;
       hc.pairs_valid = true;
+      hc.pairs_dev_off = -1;
     }
-    pairs.insert(pairs.end(), hc.pairs_cache.begin(), hc.pairs_cache.end());
+    npairs_total += (int64_t)hc.pairs_cache.size() / 2;
   }
-  npairs = (int64_t)pairs.size() / 2;
+  npairs = npairs_total;
 
   // -- device descriptors (dead blocks keep an empty descriptor)
   h_dblocks_.assign(blocks.size(), DevBlock());
@@ -1083,24 +1153,19 @@ int Engine::plan() {
     cases[ci].fresh = false;
     cases[ci].dt_stale = true;
   }
-  // cell offsets within a role slab stay below 2^31 (a slab of 2^31 cells
-  // would take 344 GB in the 4 roles, twice the HBM): 8 bytes per pair.
-  // Checked before the old descriptors are released.
-  if (cap_ >= ((int64_t)1 << 31)) return fail(FVM_ERR_INVALID, "arena too large for 32-bit ghost offsets");
   // Descriptor buffers grow (never shrink) across re-plans, so admitting or
   // retiring a case between steps costs no cudaFree / cudaMalloc (which
   // would synchronise the device) unless a buffer must grow; a growth frees
   // the old buffer and clears its pointer first, so a failed allocation
   // leaves a null member, never a freed address.
   planned_ = false;
-  std::vector<int32_t> pairs32(pairs.begin(), pairs.end());
   ncounters_ = max_stages_ * (int)groups.size();
   CK(grow_buf(&d_blocks_, &cap_blocks_, blocks.size()));
   CK(grow_buf(&d_cases_, &cap_cases_, cases.size()));
   CK(grow_buf(&d_case_blk_, &cap_case_blk_, case_blk.size()));
   CK(grow_buf(&d_tasks_, &cap_tasks_, tasks.size()));
   CK(grow_buf(&d_partials_, &cap_partials_, kPartStride * std::max<size_t>(1, tasks.size())));
-  CK(grow_buf(&d_pairs_, &cap_pairs_, std::max<size_t>(2, pairs32.size())));
+  CK(grow_buf(&d_pairs_alt_, &cap_pairs_alt_, std::max<size_t>(2, 2 * (size_t)npairs)));
   CK(grow_buf(&d_counters_, &cap_counters_, (size_t)std::max(1, ncounters_)));
   CK(grow_buf(&d_casemax_, &cap_casemax_, cases.size()));
   CK(cudaMemcpyAsync(d_blocks_, h_dblocks_.data(), sizeof(DevBlock) * blocks.size(), cudaMemcpyHostToDevice, stream));
@@ -1109,48 +1174,85 @@ int Engine::plan() {
     CK(cudaMemcpyAsync(d_case_blk_, case_blk.data(), sizeof(int) * case_blk.size(), cudaMemcpyHostToDevice, stream));
   if (!tasks.empty())
     CK(cudaMemcpyAsync(d_tasks_, tasks.data(), sizeof(Task) * tasks.size(), cudaMemcpyHostToDevice, stream));
-  if (!pairs.empty())
-    CK(cudaMemcpyAsync(d_pairs_, pairs32.data(), sizeof(int32_t) * pairs32.size(), cudaMemcpyHostToDevice, stream));
+  // the pair array is assembled on the device: a case already there moves
+  // by a device copy, only a new case's pairs cross from the host (the
+  // offsets are taken over once every copy is enqueued)
+  {
+    std::vector<int64_t> offs(live_cases.size(), -1);
+    int64_t off = 0;
+    for (size_t i = 0; i < live_cases.size(); ++i) {
+      const HCase& hc = cases[live_cases[i]];
+      const int64_t n = (int64_t)hc.pairs_cache.size();
+      if (n == 0) continue;
+      if (hc.pairs_dev_off >= 0)
+        CK(cudaMemcpyAsync(d_pairs_alt_ + off, d_pairs_ + hc.pairs_dev_off, sizeof(int32_t) * n,
+                           cudaMemcpyDeviceToDevice, stream));
+      else
+        CK(cudaMemcpyAsync(d_pairs_alt_ + off, hc.pairs_cache.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice,
+                           stream));
+      offs[i] = off;
+      off += n;
+    }
+    for (size_t i = 0; i < live_cases.size(); ++i) cases[live_cases[i]].pairs_dev_off = offs[i];
+    std::swap(d_pairs_, d_pairs_alt_);
+    std::swap(cap_pairs_, cap_pairs_alt_);
+  }
   CK(cudaMemsetAsync(d_counters_, 0, sizeof(int) * std::max(1, ncounters_), stream));
   CK(cudaMemsetAsync(d_partials_, 0, sizeof(double) * kPartStride * std::max<size_t>(1, tasks.size()), stream));
 
   // -- tensor maps of the groups whose kernel prefetches with TMA: per block
   //    and input role (A, B, C), the plane box and the z box over the block's
   //    padded box as a 4D tensor (x, y, z, variable)
-  for (auto p : d_tmap_)
-    if (p) cudaFree(p);
-  d_tmap_.assign(groups.size(), nullptr);
+  //    (grow-only device buffers, one per group slot; a block's maps are
+  //    encoded once for its arena place and box shape and kept across
+  //    re-plans, so admitting a case encodes only its own blocks)
+  if (d_tmap_.size() < groups.size()) {
+    d_tmap_.resize(groups.size(), nullptr);
+    cap_tmap_.resize(groups.size(), 0);
+  }
   if (!d_err_) CK(cudaMalloc(&d_err_, sizeof(int32_t)));
   CK(cudaMemsetAsync(d_err_, 0, sizeof(int32_t), stream));
+  std::vector<CUtensorMap> maps;
   for (size_t g = 0; g < groups.size(); ++g) {
     const Group& G = groups[g];
     if (!G.k.tma) continue;
     PFN_cuTensorMapEncodeTiled enc = encode_fn();
     if (!enc) return fail(FVM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    std::vector<CUtensorMap> maps(blocks.size() * NROLE * 2);
+    maps.assign(blocks.size() * NROLE * 2, CUtensorMap());
     std::memset(maps.data(), 0, sizeof(CUtensorMap) * maps.size());
     for (int ci : live_cases) {
       if (cases[ci].group != (int)g) continue;
       for (int bi : cases[ci].blocks) {
-        const HBlock& b = blocks[bi];
-        const cuuint64_t dims[4] = {(cuuint64_t)b.px, (cuuint64_t)b.py, (cuuint64_t)b.pz, 5};
-        const cuuint64_t strides[3] = {(cuuint64_t)(b.sy * 8), (cuuint64_t)(b.sz * 8), (cuuint64_t)(cap_ * 8)};
-        const cuuint32_t box_p[4] = {(cuuint32_t)G.k.box_w, (cuuint32_t)G.k.box_h, 1, 5};
-        const cuuint32_t box_z[4] = {(cuuint32_t)G.k.tx, (cuuint32_t)G.k.ty, 1, 5};
-        const cuuint32_t estr[4] = {1, 1, 1, 1};
-        for (int r = 0; r < NROLE; ++r) {
-          void* base = role_[r] + b.slab_off;
-          for (int w = 0; w < 2; ++w) {
-            const CUresult e = enc(&maps[((size_t)bi * NROLE + r) * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
-                                   strides, w == 0 ? box_p : box_z, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            if (e != CUDA_SUCCESS) return fail(FVM_ERR_CUDA, "cuTensorMapEncodeTiled failed for a block");
+        HBlock& b = blocks[bi];
+        const int64_t key[4] = {(int64_t)(uintptr_t)role_[0], cap_, b.slab_off,
+                                (int64_t)G.k.box_w | ((int64_t)G.k.box_h << 16) | ((int64_t)G.k.tx << 32) |
+                                    ((int64_t)G.k.ty << 48)};
+        if (b.tmaps.size() != (size_t)NROLE * 2 || !std::equal(key, key + 4, b.tmap_key)) {
+          b.tmaps.assign((size_t)NROLE * 2, CUtensorMap());
+          const cuuint64_t dims[4] = {(cuuint64_t)b.px, (cuuint64_t)b.py, (cuuint64_t)b.pz, 5};
+          const cuuint64_t strides[3] = {(cuuint64_t)(b.sy * 8), (cuuint64_t)(b.sz * 8), (cuuint64_t)(cap_ * 8)};
+          const cuuint32_t box_p[4] = {(cuuint32_t)G.k.box_w, (cuuint32_t)G.k.box_h, 1, 5};
+          const cuuint32_t box_z[4] = {(cuuint32_t)G.k.tx, (cuuint32_t)G.k.ty, 1, 5};
+          const cuuint32_t estr[4] = {1, 1, 1, 1};
+          for (int r = 0; r < NROLE; ++r) {
+            void* base = role_[r] + b.slab_off;
+            for (int w = 0; w < 2; ++w) {
+              const CUresult e = enc(&b.tmaps[(size_t)r * 2 + w], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+                                     strides, w == 0 ? box_p : box_z, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+              if (e != CUDA_SUCCESS) {
+                b.tmaps.clear();
+                return fail(FVM_ERR_CUDA, "cuTensorMapEncodeTiled failed for a block");
+              }
+            }
           }
+          std::copy(key, key + 4, b.tmap_key);
         }
+        std::copy(b.tmaps.begin(), b.tmaps.end(), maps.begin() + (size_t)bi * NROLE * 2);
       }
     }
-    CK(cudaMalloc(&d_tmap_[g], sizeof(CUtensorMap) * maps.size()));
+    CK(grow_buf(&d_tmap_[g], &cap_tmap_[g], maps.size()));
     CK(cudaMemcpyAsync(d_tmap_[g], maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, stream));
   }
   CK(cudaStreamSynchronize(stream));

@@ -48,6 +48,11 @@ struct HBlock {
   int64_t org = 0;        // offset of real cell (0,0,0) inside the padded box
   int64_t sy = 0, sz = 0;
   double* rhs_dev = nullptr;
+  // tensor maps of this block ([role][plane box, z box]), encoded for the
+  // arena base, slab offset and box shape in tmap_key; re-plans that keep
+  // those reuse them instead of encoding again
+  std::vector<CUtensorMap> tmaps;
+  int64_t tmap_key[4] = {-1, -1, -1, -1};
 };
 
 struct HCase {
@@ -61,9 +66,12 @@ struct HCase {
   int zchunk = 0;       // forced z chunk, 0 = chosen by the queue cost model over the case's group
   int tail_split = 1;   // pieces each task of the last, partial queue round is cut into (1 = none)
   // ghost gather pairs of this case, valid while its blocks keep the arena
-  // offsets in pairs_key (topology edits clear pairs_valid)
-  std::vector<int64_t> pairs_cache, pairs_key;
+  // offsets in pairs_key (topology edits clear pairs_valid); pairs_dev_off is
+  // where they sit in the engine's device pair array (-1: not there)
+  std::vector<int32_t> pairs_cache;
+  std::vector<int64_t> pairs_key;
   bool pairs_valid = false;
+  int64_t pairs_dev_off = -1;
 };
 
 struct Group {
@@ -116,6 +124,10 @@ class Engine {
   cudaStream_t stream = nullptr;
   int device = 0;
   int num_sms = 148;
+  // resident CTAs per SM of each stage kernel at its shared-memory size,
+  // found once (the attribute and the occupancy query cost a driver call
+  // each, on every re-plan otherwise)
+  std::vector<std::pair<const void*, int>> occ_cache_;
   std::vector<HCase> cases;
   std::vector<HBlock> blocks;
   std::vector<Group> groups;
@@ -171,17 +183,20 @@ class Engine {
   Task* d_tasks_ = nullptr;
   double* d_partials_ = nullptr;
   int32_t* d_pairs_ = nullptr;       // (dst, src) cell offsets within a role slab
+  int32_t* d_pairs_alt_ = nullptr;   // the next plan's pair array, assembled on the device
   int* d_counters_ = nullptr;
   int ncounters_ = 0;
   // viscous task lists in d_tasks_, index precision * 2 + (3D ? 0 : 1)
   int vlist_off_[6] = {0, 0, 0, 0, 0, 0}, vlist_n_[6] = {0, 0, 0, 0, 0, 0};
   std::vector<CUtensorMap*> d_tmap_;  // per group: [block][role A..ACC][plane, z] (null: no TMA)
+  std::vector<size_t> cap_tmap_;      // their capacities in maps (grown, never shrunk)
   int32_t* d_err_ = nullptr;          // kernel error flag (a tensor copy that did not arrive)
   int* d_dtmask_ = nullptr;           // cases whose dt prepare() recomputes
   int dtmask_cap_ = 0;
   bool drop_copies_ = false;          // test hook: tensor copies armed but not issued
   unsigned long long* d_casemax_ = nullptr;
   // element capacities of the descriptor buffers above (grown, never shrunk)
+  size_t cap_pairs_alt_ = 0;
   size_t cap_blocks_ = 0, cap_cases_ = 0, cap_case_blk_ = 0, cap_tasks_ = 0, cap_partials_ = 0, cap_pairs_ = 0,
          cap_counters_ = 0, cap_casemax_ = 0;
   double* d_staging_ = nullptr;
