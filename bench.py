@@ -46,6 +46,14 @@ STAGE_TRAFFIC = {(1, 3, 32, 4): 366.8e6, (2, 2, 16, 2): 365.7e6}
 # the same kernel configuration as its ncu capture (--autotune searches
 # again). Precision ids: 1 FP64, 2 FP32 flux.
 FIXED_TILING = {1: (3, 32, 4), 2: (2, 16, 2)}
+# The arithmetic roof beside the HBM one: the stage kernel's busiest
+# instruction pipe for the fixed tilings: the fraction of the kernel's active
+# cycles that pipe was busy (ncu
+# sm__pipe_<pipe>_cycles_active.avg.pct_of_peak_sustained_active, mean of the
+# first two stages of a step); the FP64 form is bound by the FP64 pipe, the
+# FP32-flux form by the FMA pipe (its WENO runs in f32x2 instructions, two
+# pipe cycles each)
+STAGE_PIPE = {(1, 3, 32, 4): ("fp64", 0.574), (2, 2, 16, 2): ("fma", 0.426)}
 WORKLOAD = "isentropic vortex 3D Euler, periodic [-5,5]^3, 8 uneven blocks, 128^3 = 2,097,152 cells, WENO5 + AUSM, RK4, CFL 0.5"
 
 
@@ -304,11 +312,14 @@ def product(args, dist: Dist):
         ach = alg / (per_step_ms * 1e-3) / 1e9
         pk = peaks()
         share = per_step_ms / (sum(ms for p in prof for _, ms in p) / len(prof))
-        traffic = STAGE_TRAFFIC.get((prec,) + tuple(r["tiling"])) if args.n == 128 else None
+        key = (prec,) + tuple(r["tiling"])
+        traffic = STAGE_TRAFFIC.get(key) if args.n == 128 else None
+        pipe = STAGE_PIPE.get(key) if args.n == 128 else None
         return {"bound": "hbm", "achieved": sig(ach), "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": sig(ach / pk["hbm_gbs"]), "traffic": traffic, "peak_src": pk["src"],
                 "kernel": "stage_kernel", "stage_ms_per_step": sig(per_step_ms), "stage_share_of_step": sig(share),
-                "alg_bytes_per_cell_step": 640, "alg_bytes_per_launch": round(160.0 * ncells)}
+                "alg_bytes_per_cell_step": 640, "alg_bytes_per_launch": round(160.0 * ncells),
+                "alu_roof": ({"pipe": pipe[0], "busy_of_peak": pipe[1], "src": "ncu"} if pipe else None)}
 
     forms = args.forms.split(",")
     runs = {}
@@ -341,7 +352,7 @@ def product(args, dist: Dist):
                "spread_ms": [sig(min(r["win"])), sig(max(r["win"]))]}
         if f == "fp32":
             rec["roofline"] = {k: v for k, v in roof(r, r["prec"]).items()
-                               if k in ("achieved", "frac", "traffic", "stage_ms_per_step")}
+                               if k in ("achieved", "frac", "traffic", "stage_ms_per_step", "alu_roof")}
             ref = "fp64" if "fp64" in runs else ("exact" if "exact" in runs else None)
             if ref:
                 rec["l1_density_vs_" + ref] = sig(l1rho(f, ref))
