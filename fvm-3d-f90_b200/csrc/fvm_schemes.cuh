@@ -96,6 +96,18 @@ __device__ __forceinline__ Prim5<R> cons2prim(R q0, R q1, R q2, R q3, R q4, R gm
   }
   return s;
 }
+// The non-exact conversion that also returns 1 / rho.
+template <class R>
+__device__ __forceinline__ Prim5<R> cons2prim_ir(R q0, R q1, R q2, R q3, R q4, R gm1, R& ir) {
+  Prim5<R> s;
+  s.r = q0;
+  ir = rcp_(q0);
+  s.u = q1 * ir;
+  s.v = q2 * ir;
+  s.w = q3 * ir;
+  s.p = gm1 * (q4 - R(0.5) * (q1 * s.u + q2 * s.v + q3 * s.w));
+  return s;
+}
 
 // ------------------------------------------------------------ MUSCL
 // scheme_reconstruct_MUSCL.f90:114-226. Limited differences of the centre
@@ -513,6 +525,56 @@ __device__ __forceinline__ void flux_ausm(const Prim5<R>& L, const Prim5<R>& Rs,
   F[3] = wl * (phl * L.w) + wr * (phr * Rs.w);
   F[1 + DIR] = F[1 + DIR] + p_;
   F[4] = wl * (phl * H_l) + wr * (phr * H_r);
+}
+
+// AUSM on precomputed sides (non-exact forms). In the reference's WENO
+// variant a node's reconstructed state is the left state of one face and the
+// right state of the next, so what AUSM derives from one side alone (1/rho,
+// H, c, the normal Mach number, rho c) is formed once per node by ausm_side
+// instead of once per face and side; flux_ausm_sides is then the !EX branch
+// of flux_ausm with those values, operation for operation.
+template <class R> struct AusmSide { R u, v, w, p, H, M, rc; };
+
+// s: the node's primitive state, ir = 1 / s.r (as cons2prim formed it),
+// Vc: its velocity along the face normal.
+template <class R>
+__device__ __forceinline__ AusmSide<R> ausm_side(const Prim5<R>& s, R ir, R Vc, const SchemeConst<R>& k) {
+  AusmSide<R> o;
+  const R pr = s.p * ir;
+  o.u = s.u;
+  o.v = s.v;
+  o.w = s.w;
+  o.p = s.p;
+  o.H = k.goverg1 * pr + R(0.5) * (s.u * s.u + s.v * s.v + s.w * s.w);
+  const R a = k.gamma * pr;
+  const R rs = rsqrt_(a);
+  o.M = Vc * rs;
+  o.rc = s.r * (a * rs);
+  return o;
+}
+
+template <int DIR, class R>
+__device__ __forceinline__ void flux_ausm_sides(const AusmSide<R>& L, const AusmSide<R>& Rs, R F[5]) {
+  const R M_l = L.M, M_r = Rs.M;
+  const bool sup_l = abs_(M_l) >= R(1.0), sup_r = abs_(M_r) >= R(1.0);
+  const R hl = M_l + R(1.0), hr = M_r - R(1.0);
+  const R msub_l = (R(0.25) * hl) * hl, msub_r = (R(0.25) * hr) * hr;
+  const R ms_l = sup_l ? fmax(M_l, R(0)) : msub_l;
+  const R ms_r = sup_r ? fmin(M_r, R(0)) : -msub_r;
+  const R ps_l = sup_l ? (M_l > R(0) ? R(1) : R(0)) : msub_l * (R(2.0) - M_l);
+  const R ps_r = sup_r ? (M_r < R(0) ? R(1) : R(0)) : msub_r * (R(2.0) + M_r);
+  const R Mn = ms_l + ms_r;
+  const R am = abs_(Mn);
+  const R Mabs = (am > R(0.1)) ? am : (am * am + R(0.01)) * R(5.0);
+  const R p_ = ps_l * L.p + ps_r * Rs.p;
+  const R gl = (R(0.5) * (Mn + Mabs)) * L.rc;
+  const R gr = (R(0.5) * (Mn - Mabs)) * Rs.rc;
+  F[0] = gl + gr;
+  F[1] = gl * L.u + gr * Rs.u;
+  F[2] = gl * L.v + gr * Rs.v;
+  F[3] = gl * L.w + gr * Rs.w;
+  F[1 + DIR] = F[1 + DIR] + p_;
+  F[4] = gl * L.H + gr * Rs.H;
 }
 
 template <int FLUX, int DIR, class R, bool EX>

@@ -28,6 +28,8 @@
 #pragma once
 #include <cuda_pipeline.h>
 
+#include <type_traits>
+
 #include "fvm_schemes.cuh"
 #include "fvm_types.h"
 
@@ -46,7 +48,12 @@ struct StageCfg {
   static constexpr int PW = TX + 2 * H, PH = TY + 2 * H;
   // node values per x / y node item: WENO 5 (left-biased) or 10 (both
   // sides); MUSCL 10 (the cell's values at its right and left faces)
-  static constexpr int NODEV = RECON == RECON_WENO_ ? (TB ? 10 : 5) : (RECON == RECON_MUSCL_ ? 10 : 0);
+  // AUSM on per-node sides (ausm_side): the reference's WENO variant, whose
+  // node value is the left state of one face and the right state of the
+  // next, with AUSM in a non-exact form; a node then stores the seven values
+  // of AusmSide instead of its five primitives
+  static constexpr bool SP = RECON == RECON_WENO_ && !TB && FLUX == FLUX_AUSM_ && !EX;
+  static constexpr int NODEV = RECON == RECON_WENO_ ? (TB ? 10 : (SP ? 7 : 5)) : (RECON == RECON_MUSCL_ ? 10 : 0);
   static constexpr int NXN = (TX + 2) * TY, NYN = TX * (TY + 2);
   static constexpr int NXF = (TX + 1) * TY, NYF = TX * (TY + 1);
   static constexpr int NW = 2 * H * (TX + TY);             // halo cells of a plane
@@ -468,7 +475,9 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
 
     // ---- z window (3D) --------------------------------------------------
     R zw[C::WIN][5];
-    Prim5<R> zWprev;       // WENO: node value of plane k (ref: left-biased; TB: minus side)
+    // a node's face state: primitives, or with SP the AUSM side values
+    using NodeT = std::conditional_t<C::SP, AusmSide<R>, Prim5<R>>;
+    NodeT zWprev;          // WENO: node value of plane k (ref: left-biased; TB: minus side)
     R zFprev[5] = {0, 0, 0, 0, 0};
     const int kstart = (DIM == 3) ? T.z0 - C::WZ : T.z0;
     if constexpr (DIM == 3) {
@@ -573,7 +582,19 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       }
 
       // ---- phase A: WENO nodes --------------------------------------------
-      Prim5<R> zWcur, zWm_cur;
+      NodeT zWcur, zWm_cur;
+      constexpr int NNODE = C::NXN + C::NYN;
+      // SP: the side values of x / y node w from its primitives and 1 / rho
+      auto store_side = [&](int w, const Prim5<R>& pm, R ir) {
+        const AusmSide<R> sd = ausm_side<R>(pm, ir, w < C::NXN ? pm.u : pm.v, K);
+        sN[0 * NNODE + w] = sd.u;
+        sN[1 * NNODE + w] = sd.v;
+        sN[2 * NNODE + w] = sd.w;
+        sN[3 * NNODE + w] = sd.p;
+        sN[4 * NNODE + w] = sd.H;
+        sN[5 * NNODE + w] = sd.M;
+        sN[6 * NNODE + w] = sd.rc;
+      };
       if constexpr (RECON == RECON_WENO_) {
         if constexpr (sizeof(R) == 4 && !TB) {
           // FP32, left-biased nodes only. A node's five variables fill two and
@@ -612,6 +633,12 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             wm[3] = r23.y;
           };
           auto finish = [&](int w, const R (&u)[5][5], const R (&wm)[5]) {
+            if constexpr (C::SP) {
+              R ir;
+              const Prim5<R> pm = cons2prim_ir<R>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1, ir);
+              store_side(w, pm, ir);
+              return;
+            }
             Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
             if (K.textbook && !admissible(pm))
               pm = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
@@ -672,11 +699,18 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           }
           if (hz) {
             if (!zpaired) wz[4] = pair(uz4, uz4).x;
-            zWm_cur = cons2prim<R, EX>(wz[0], wz[1], wz[2], wz[3], wz[4], K.gm1);
-            zWcur = zWm_cur;
-            if (K.textbook && !admissible(zWm_cur)) {
-              zWm_cur = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
+            if constexpr (C::SP) {
+              R ir;
+              const Prim5<R> pz = cons2prim_ir<R>(wz[0], wz[1], wz[2], wz[3], wz[4], K.gm1, ir);
+              zWm_cur = ausm_side<R>(pz, ir, pz.w, K);
               zWcur = zWm_cur;
+            } else {
+              zWm_cur = cons2prim<R, EX>(wz[0], wz[1], wz[2], wz[3], wz[4], K.gm1);
+              zWcur = zWm_cur;
+              if (K.textbook && !admissible(zWm_cur)) {
+                zWm_cur = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
+                zWcur = zWm_cur;
+              }
             }
           }
           if (do_xy) __syncthreads();
@@ -689,6 +723,12 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
 #pragma unroll
             for (int s = 0; s < 5; ++s) u[v][s] = zw[s][v];
           weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
+          if constexpr (C::SP) {
+            R ir;
+            const Prim5<R> pz = cons2prim_ir<R>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1, ir);
+            zWm_cur = ausm_side<R>(pz, ir, pz.w, K);
+            zWcur = zWm_cur;
+          } else {
           zWm_cur = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
           if (TB)
             zWcur = cons2prim<R, EX>(wp[0], wp[1], wp[2], wp[3], wp[4], K.gm1);
@@ -698,6 +738,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             const Prim5<R> pc = cons2prim<R, EX>(zw[2][0], zw[2][1], zw[2][2], zw[2][3], zw[2][4], K.gm1);
             if (!admissible(zWm_cur)) zWm_cur = pc;
             if (!admissible(zWcur)) zWcur = pc;
+          }
           }
         }
         if (do_xy) {
@@ -721,6 +762,12 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             }
             R wm[5], wp[5];
             weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
+            if constexpr (C::SP) {
+              R ir;
+              const Prim5<R> pm = cons2prim_ir<R>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1, ir);
+              store_side(w, pm, ir);
+              continue;
+            }
             Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
             if (K.textbook && !admissible(pm))
               pm = cons2prim<R, EX>(u[0][2], u[1][2], u[2][2], u[3][2], u[4][2], K.gm1);
@@ -813,23 +860,49 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       R zF[5] = {0, 0, 0, 0, 0};
       if constexpr (DIM == 3) {
         if (colt && k >= T.z0 - 1) {
-          Prim5<R> L, Rr;
-          if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
-            L = zWprev;
-            Rr = zWcur;
+          if constexpr (C::SP) {
+            flux_ausm_sides<2, R>(zWprev, zWcur, zF);
           } else {
-            L = mkprim(zw[1]);
-            Rr = mkprim(zw[2]);
+            Prim5<R> L, Rr;
+            if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
+              L = zWprev;
+              Rr = zWcur;
+            } else {
+              L = mkprim(zw[1]);
+              Rr = mkprim(zw[2]);
+            }
+            face_flux<FLUX, 2, R, EX>(L, Rr, K, zF);
           }
-          face_flux<FLUX, 2, R, EX>(L, Rr, K, zF);
         }
       }
       if (do_xy) {
         constexpr int NN = C::NXN + C::NYN;
         constexpr int NF = C::NXF + C::NYF;
+        auto load_side = [&](int n) {
+          AusmSide<R> sd;
+          sd.u = sN[0 * NN + n];
+          sd.v = sN[1 * NN + n];
+          sd.w = sN[2 * NN + n];
+          sd.p = sN[3 * NN + n];
+          sd.H = sN[4 * NN + n];
+          sd.M = sN[5 * NN + n];
+          sd.rc = sN[6 * NN + n];
+          return sd;
+        };
         for (int w = tid; w < NF; w += NT) {
           R F[5];
-          if (w < C::NXF) {
+          if constexpr (C::SP) {
+            if (w < C::NXF) {
+              const int f = w % (TX + 1), row = w / (TX + 1);
+              const int nl = row * (TX + 2) + f;
+              flux_ausm_sides<0, R>(load_side(nl), load_side(nl + 1), F);
+            } else {
+              const int w2 = w - C::NXF;
+              const int col = w2 % TX, f = w2 / TX;
+              const int nl = C::NXN + f * TX + col;
+              flux_ausm_sides<1, R>(load_side(nl), load_side(nl + TX), F);
+            }
+          } else if (w < C::NXF) {
             const int f = w % (TX + 1), row = w / (TX + 1);
             Prim5<R> L, Rr;
             if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
