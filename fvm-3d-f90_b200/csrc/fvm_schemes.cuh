@@ -38,19 +38,20 @@ template <class R> struct SchemeConst {
 // rcp_ / rsqrt_ / nsqrt_ serve the non-exact forms only (the exact form
 // divides and takes IEEE square roots in the reference's order). In FP64
 // they start from the hardware approximation (rcp / rsqrt .approx.ftz.f64)
-// and take two Newton-Raphson steps, r <- r + r (1 - x r) and
-// y <- y + y (1 - x y^2) / 2, each of which squares the relative error, so
-// the result is within a couple of ulp of the correctly rounded one with no
-// special-case branch. Arguments are positive normal numbers (densities,
-// pressures, squared sound speeds, limiter and entropy-fix denominators);
-// a zero argument gives a non-finite result, as the exact division does.
+// and take one third-order correction: with e = 1 - x r (reciprocal) or
+// e = 1 - x y^2 (reciprocal square root), r (1 + e + e^2) = (1 - e^3) / x
+// and y (1 + e/2 + 3e^2/8) = x^(-1/2) (1 + O(e^3)), so the approximation's
+// relative error is cubed in three (reciprocal) or five (reciprocal square
+// root) FP64 operations, and the result is within a couple of ulp of the
+// correctly rounded one with no special-case branch. Arguments are positive
+// normal numbers (densities, pressures, squared sound speeds, limiter and
+// entropy-fix denominators); a zero argument gives a non-finite result, as
+// the exact division does.
 __device__ __forceinline__ double rcp_(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  double e = fma(-x, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-x, r, 1.0);
-  return fma(r, e, r);
+  const double e = fma(-x, r, 1.0);
+  return fma(r, fma(e, e, e), r);
 }
 __device__ __forceinline__ float rcp_(float x) { return __fdividef(1.0f, x); }
 __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
@@ -58,10 +59,8 @@ __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
 __device__ __forceinline__ double rsqrt_(double x) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-(x * y), y, 1.0);
-  y = fma(0.5 * y, e, y);
-  e = fma(-(x * y), y, 1.0);
-  return fma(0.5 * y, e, y);
+  const double e = fma(-(x * y), y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
 }
 __device__ __forceinline__ float rsqrt_(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double nsqrt_(double x) { return x * rsqrt_(x); }
@@ -173,7 +172,10 @@ __device__ __forceinline__ R weno5(R u0, R u1, R u2, R u3, R u4, int textbook) {
     // smoothness indicators and eps are scaled by 4 (the weights only see
     // their ratios): 4 (IS_k + eps) = 13/3 a_k^2 + b_k^2 + 4e-6. The weights
     // are division-free, omega_k = c_k prod_{j!=k} d_j / D with d = e^2, and
-    // the result is u2 + sum omega_k delta_k.
+    // the result is u2 + sum omega_k delta_k. With P0 = d1 d2, P1 = d0 d2
+    // and P2 = d0 d1 / 2 the weights are (P0, 6 P1, 6 P2) / (P0 + 6 (P1 + P2)),
+    // so the constants of the linear weights fold into 6 delta_1 =
+    // D12 + 2 D23 and 6 delta_2 = 4 D23 - D34 (one operation each).
     const R D01 = u1 - u0, D12 = u2 - u1, D23 = u3 - u2, D34 = u4 - u3;
     const R a0 = D12 - D01, a1 = D23 - D12, a2 = D34 - D23;
     const R b0 = R(2.0) * D12 + a0;
@@ -183,13 +185,11 @@ __device__ __forceinline__ R weno5(R u0, R u1, R u2, R u3, R u4, int textbook) {
     const R e1 = (R(13.0 / 3.0) * a1) * a1 + (b1 * b1 + R(4.0e-6));
     const R e2 = (R(13.0 / 3.0) * a2) * a2 + (b2 * b2 + R(4.0e-6));
     const R d0 = e0 * e0, d1 = e1 * e1, d2 = e2 * e2;
-    const R t0 = d1 * d2;
-    const R t1 = (R(6.0) * d0) * d2;
-    const R t2 = (R(3.0) * d0) * d1;
-    const R s0 = R(5.0 / 6.0) * D12 + R(-1.0 / 3.0) * D01;
-    const R s1 = R(1.0 / 3.0) * D23 + R(1.0 / 6.0) * D12;
-    const R s2 = R(2.0 / 3.0) * D23 + R(-1.0 / 6.0) * D34;
-    return (t0 * s0 + (t1 * s1 + t2 * s2)) * rcp_(t0 + (t1 + t2)) + u2;
+    const R P0 = d1 * d2, P1 = d0 * d2, P2 = (R(0.5) * d0) * d1;
+    const R s0 = R(1.0 / 3.0) * b0 + R(-1.0 / 6.0) * D12;  // delta_0 = (2 b0 - D12) / 6
+    const R S1 = R(2.0) * D23 + D12;
+    const R S2 = R(4.0) * D23 - D34;
+    return (P0 * s0 + (P1 * S1 + P2 * S2)) * rcp_(R(6.0) * (P1 + P2) + P0) + u2;
   }
 }
 
@@ -211,15 +211,16 @@ __device__ __forceinline__ float2 weno5x2(float2 u0, float2 u1, float2 u2, float
   const float2 e1 = __ffma2_rn(__fmul2_rn(c, a1), a1, __ffma2_rn(b1, b1, eps));
   const float2 e2 = __ffma2_rn(__fmul2_rn(c, a2), a2, __ffma2_rn(b2, b2, eps));
   const float2 d0 = __fmul2_rn(e0, e0), d1 = __fmul2_rn(e1, e1), d2 = __fmul2_rn(e2, e2);
-  // weights c_k / d_k normalised by 1 / c_0: t0 = d1 d2, t1 = 6 d0 d2, t2 = 3 d0 d1
-  const float2 t0 = __fmul2_rn(d1, d2);
-  const float2 t1 = __fmul2_rn(__fmul2_rn(f2_(6.0f), d0), d2);
-  const float2 t2 = __fmul2_rn(__fmul2_rn(f2_(3.0f), d0), d1);
-  const float2 s0 = __ffma2_rn(f2_(5.0f / 6.0f), D12, __fmul2_rn(f2_(-1.0f / 3.0f), D01));
-  const float2 s1 = __ffma2_rn(f2_(1.0f / 3.0f), D23, __fmul2_rn(f2_(1.0f / 6.0f), D12));
-  const float2 s2 = __ffma2_rn(f2_(2.0f / 3.0f), D23, __fmul2_rn(f2_(-1.0f / 6.0f), D34));
-  const float2 num = __ffma2_rn(t0, s0, __ffma2_rn(t1, s1, __fmul2_rn(t2, s2)));
-  const float2 den = __fadd2_rn(t0, __fadd2_rn(t1, t2));
+  // weights c_k / d_k normalised by 1 / c_0, with the constants of c_1 and
+  // c_2 folded into the differences (the FP64 form's P0, P1, P2, S1, S2)
+  const float2 P0 = __fmul2_rn(d1, d2);
+  const float2 P1 = __fmul2_rn(d0, d2);
+  const float2 P2 = __fmul2_rn(__fmul2_rn(f2_(0.5f), d0), d1);
+  const float2 s0 = __ffma2_rn(f2_(1.0f / 3.0f), b0, __fmul2_rn(f2_(-1.0f / 6.0f), D12));
+  const float2 S1 = __ffma2_rn(f2_(2.0f), D23, D12);
+  const float2 S2 = __ffma2_rn(m1, b2, D23);  // 4 D23 - D34
+  const float2 num = __ffma2_rn(P0, s0, __ffma2_rn(P1, S1, __fmul2_rn(P2, S2)));
+  const float2 den = __ffma2_rn(f2_(6.0f), __fadd2_rn(P1, P2), P0);
   return __ffma2_rn(num, make_float2(rcp_(den.x), rcp_(den.y)), u2);
 }
 

@@ -93,7 +93,7 @@ def test_error_paths():
 
 def test_fast_fp64_reciprocals_within_2ulp():
     # the non-exact FP64 forms' reciprocal and reciprocal square root
-    # (hardware approximation + two Newton-Raphson steps) against correctly
+    # (hardware approximation + one third-order correction) against correctly
     # rounded references (long double), over normal arguments whose results
     # are normal too
     import ctypes
