@@ -585,8 +585,8 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       NodeT zWcur, zWm_cur;
       constexpr int NNODE = C::NXN + C::NYN;
       // SP: the side values of x / y node w from its primitives and 1 / rho
-      auto store_side = [&](int w, const Prim5<R>& pm, R ir) {
-        const AusmSide<R> sd = ausm_side<R>(pm, ir, w < C::NXN ? pm.u : pm.v, K);
+      auto store_side = [&](int w, const Prim5<R>& pm, R ir, R E) {
+        const AusmSide<R> sd = ausm_side<R>(pm, ir, E, w < C::NXN ? pm.u : pm.v, K);
         sN[0 * NNODE + w] = sd.u;
         sN[1 * NNODE + w] = sd.v;
         sN[2 * NNODE + w] = sd.w;
@@ -636,7 +636,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             if constexpr (C::SP) {
               R ir;
               const Prim5<R> pm = cons2prim_ir<R>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1, ir);
-              store_side(w, pm, ir);
+              store_side(w, pm, ir, wm[4]);
               return;
             }
             Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
@@ -702,7 +702,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             if constexpr (C::SP) {
               R ir;
               const Prim5<R> pz = cons2prim_ir<R>(wz[0], wz[1], wz[2], wz[3], wz[4], K.gm1, ir);
-              zWm_cur = ausm_side<R>(pz, ir, pz.w, K);
+              zWm_cur = ausm_side<R>(pz, ir, wz[4], pz.w, K);
               zWcur = zWm_cur;
             } else {
               zWm_cur = cons2prim<R, EX>(wz[0], wz[1], wz[2], wz[3], wz[4], K.gm1);
@@ -726,7 +726,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           if constexpr (C::SP) {
             R ir;
             const Prim5<R> pz = cons2prim_ir<R>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1, ir);
-            zWm_cur = ausm_side<R>(pz, ir, pz.w, K);
+            zWm_cur = ausm_side<R>(pz, ir, wm[4], pz.w, K);
             zWcur = zWm_cur;
           } else {
           zWm_cur = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
@@ -765,7 +765,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             if constexpr (C::SP) {
               R ir;
               const Prim5<R> pm = cons2prim_ir<R>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1, ir);
-              store_side(w, pm, ir);
+              store_side(w, pm, ir, wm[4]);
               continue;
             }
             Prim5<R> pm = cons2prim<R, EX>(wm[0], wm[1], wm[2], wm[3], wm[4], K.gm1);
