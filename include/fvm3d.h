@@ -265,7 +265,7 @@ int fvm_kernel_launches_per_step(fvm_ctx* ctx, int* n);
  * stays usable (upload a state again after turning the hook off). */
 int fvm_test_drop_tensor_copies(fvm_ctx* ctx, int on);
 /* Test hook of the non-exact FP64 forms' reciprocal and reciprocal square
- * root (hardware approximation and two Newton-Raphson steps); no
+ * root (hardware approximation and one third-order correction); no
  * counterpart in the reference. Evaluates both over the host array x[0..n)
  * on the device into host arrays rcp_out / rsqrt_out. */
 int fvm_test_fast_math(const double* x, int64_t n, double* rcp_out, double* rsqrt_out);
