@@ -330,21 +330,27 @@ __device__ __forceinline__ void flux_roe(const Prim5<R>& L, const Prim5<R>& Rs, 
     // momentum (d1+d234+d5) u_b + lam2 rho_b du (+ (d5-d1) c_b - lam2 rho_b dV
     // along the normal) and energy (d1+d5) H_b + (d5-d1) c_b V_b
     // + d234 q2_b / 2 + lam2 rho_b (u_b . du - V_b dV)
+    // Along the normal the velocity jump is dVl itself, so lam2 rho_b (du_n
+    // - dVl) and u_b,n du_n - V_b dVl vanish: the normal momentum's
+    // dissipation is dsum u_b,n + ddif and u_b . du - V_b dV sums the two
+    // tangential terms.
     const R dsum = d1_0 + d234_0 + d5_0;
     const R ddif = (d5_0 - d1_0) * c_b;
     const R ml = L.r * Vc_l, mr = Rs.r * Vc_r;
     F[0] = R(0.5) * ((ml + mr) - dsum);
+    R ud = R(0);
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      R diss = dsum * ub[m] + l2r * dd[m];
-      R phys = ml * ul[m] + mr * ur[m];
+      R diss, phys = ml * ul[m] + mr * ur[m];
       if (m == DIR) {
-        diss = diss + (ddif - l2r * dVl);
+        diss = dsum * ub[m] + ddif;
         phys = phys + (L.p + Rs.p);
+      } else {
+        diss = dsum * ub[m] + l2r * dd[m];
+        ud = ud + ub[m] * dd[m];
       }
       F[1 + m] = R(0.5) * (phys - diss);
     }
-    const R ud = u_b * du + v_b * dv + w_b * dw - Vl_b * dVl;
     const R de = (d1_0 + d5_0) * H_b + ddif * Vl_b + d234_0 * (R(0.5) * q2_b) + l2r * ud;
     F[4] = R(0.5) * ((ml * H_l + mr * H_r) - de);
     return;
