@@ -88,6 +88,10 @@ struct StageCfg {
   // (the layout of the operand arrays), which keeps the per-thread copies
   // and their L1 lines out of the plane loop.
   static constexpr bool TMA = PSM && DIM == 3;
+  // FP64 WENO tiles with tensor copies read their node stencils straight
+  // from the plane's box (no copy into the plane array, one barrier less per
+  // plane); the next plane's box is issued once the node phase is done
+  static constexpr bool BOXA = TMA && RECON == RECON_WENO_ && sizeof(R) == 8;
   static constexpr int TW = (TX + 2 * H + 2) / 2 * 2;
   static constexpr int TPB = (5 * PH * TW + 15) / 16 * 16;
   static constexpr int TZB = (5 * TY * TX + 15) / 16 * 16;
@@ -361,6 +365,7 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
   __shared__ int s_task;
   __shared__ __align__(8) uint64_t s_mbar[3];  // TMA: plane box, z box, RK operands
   __shared__ uint64_t s_issued;                  // TMA: globaltimer when this plane's copies were issued
+  __shared__ uint64_t s_issp;                    // BOXA: globaltimer when the plane box was issued
   uint32_t ph_p = 0, ph_z = 0, ph_q = 0;       // TMA: expected phase parity of each mbarrier
 
   const int tid = threadIdx.x;
@@ -465,6 +470,16 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       xy_clamp(G, x, y);
       zsrc = (y - T.y0) * TX + (x - T.x0);
     }
+    // BOXA: plane cell (xx, yy) is box element yy * TW + xx + xoff. The box
+    // holds ghost storage where the clamped rule gives other values (halo
+    // cells of transmissive faces) and, past a partial tile's block edge,
+    // where the z window holds the clamped values: such a task fixes those
+    // cells up in the box after each plane lands.
+    const int xoff = (T.x0 + kPadX - H) - xs;
+    bool fixt = false;
+    if constexpr (C::BOXA)
+      fixt = (!(G.mask & 1) && T.x0 < H) || (!(G.mask & 2) && T.x0 + nxt + H > G.n0) ||
+             (!(G.mask & 4) && T.y0 < H) || (!(G.mask & 8) && T.y0 + nyt + H > G.n1) || nxt < TX || nyt < TY;
     // tensor maps of this block: [role][plane box, z-shaped box]
     const CUtensorMap* tmb = nullptr;
     const CUtensorMap* tmp = nullptr;
@@ -517,7 +532,9 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       if constexpr (C::TMA) {
         if (tid == 0) {
           s_issued = global_ns();  // the deadline of this plane's waits is one second later
-          if (more_xy) {
+          // (BOXA: a node plane's box for plane k+1 is issued after its node phase)
+          if (more_xy && !(C::BOXA && do_xy)) {
+            if constexpr (C::BOXA) s_issp = s_issued;
             mbar_expect_tx(&s_mbar[0], sizeof(double) * 5 * PH * C::TW);
             // a.drop_copies (a test of the timeout path): the barrier is armed
             // but the copy never issued, so the wait below runs out
@@ -741,24 +758,53 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           }
           }
         }
+        if constexpr (C::BOXA) {
+          if (do_xy) {
+            // the plane's box (issued after the last plane's node phase)
+            if (!mbar_wait(&s_mbar[0], ph_p, &s_issp)) {
+              leave_after_timeout(tid, a.err);
+              return;
+            }
+            ph_p ^= 1;
+            if (fixt) {
+#pragma unroll
+              for (int sidx = 0; sidx < C::NPS; ++sidx) {
+                if (lsp[sidx] >= 0) {
+                  const int nat = (lsp[sidx] / PW) * C::TW + lsp[sidx] % PW + xoff;
+                  if (nat != lxy[sidx])
+#pragma unroll
+                    for (int v = 0; v < 5; ++v) sTP[v * (PH * C::TW) + nat] = sTP[v * (PH * C::TW) + lxy[sidx]];
+                }
+              }
+              if (colt && (tx >= nxt || ty >= nyt))
+#pragma unroll
+                for (int v = 0; v < 5; ++v) sTP[v * (PH * C::TW) + (H + ty) * C::TW + H + tx + xoff] = zw[1][v];
+              __syncthreads();
+            }
+          }
+        }
         if (do_xy) {
+          // node stencils from the plane array, or with BOXA from the box
+          const R* pl = sP;
+          if constexpr (C::BOXA) pl = reinterpret_cast<const R*>(sTP) + xoff;
+          constexpr int PLS = C::BOXA ? PH * C::TW : PLANE, PWS = C::BOXA ? C::TW : PW;
           for (int w = tid; w < C::NXN + C::NYN; w += NT) {
             R u[5][5];
             if (w < C::NXN) {
               const int c = w % (TX + 2) - 1, row = w / (TX + 2);
-              const int base = (H + row) * PW + (H + c - 2);
+              const int base = (H + row) * PWS + (H + c - 2);
 #pragma unroll
               for (int v = 0; v < 5; ++v)
 #pragma unroll
-                for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s];
+                for (int s = 0; s < 5; ++s) u[v][s] = pl[v * PLS + base + s];
             } else {
               const int w2 = w - C::NXN;
               const int col = w2 % TX, c = w2 / TX - 1;
-              const int base = (H + c - 2) * PW + (H + col);
+              const int base = (H + c - 2) * PWS + (H + col);
 #pragma unroll
               for (int v = 0; v < 5; ++v)
 #pragma unroll
-                for (int s = 0; s < 5; ++s) u[v][s] = sP[v * PLANE + base + s * PW];
+                for (int s = 0; s < 5; ++s) u[v][s] = pl[v * PLS + base + s * PWS];
             }
             R wm[5], wp[5];
             weno5_node<R, EX, TB>(u, K.textbook, wm, wp);
@@ -788,6 +834,15 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
             }
           }
           __syncthreads();
+          if constexpr (C::BOXA) {
+            // the box is free: the next plane's copy goes out now and lands
+            // while the fluxes and the update of this plane run
+            if (tid == 0 && more_xy) {
+              s_issp = global_ns();
+              mbar_expect_tx(&s_mbar[0], sizeof(double) * 5 * PH * C::TW);
+              if (!a.drop_copies) tma_load_4d(sTP, tmp, xs, T.y0 + kGhost - H, k + 1 + kGhost, 0, &s_mbar[0]);
+            }
+          }
         }
         }
       }
@@ -1068,14 +1123,14 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
       }
 
       // ---- carry, window shift and shared-memory refill ----------------------
-      if constexpr (C::FAL) __syncthreads();
+      if constexpr (C::FAL && !C::BOXA) __syncthreads();
       if constexpr (C::PSM && !C::TMA) __pipeline_wait_prior(0);
       if constexpr (C::TMA) {
         if (more) {
           fail |= !mbar_wait(&s_mbar[1], ph_z, &s_issued);
           ph_z ^= 1;
         }
-        if (more_xy) {
+        if (more_xy && !C::BOXA) {
           fail |= !mbar_wait(&s_mbar[0], ph_p, &s_issued);
           ph_p ^= 1;
         }
@@ -1098,13 +1153,13 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           }
           to_stencil<RECON, R, EX>(zpre, zw[C::WIN - 1], gm1d, K.gm1);
         }
-        if (more_xy) {
+        if (more_xy && !C::BOXA) {
           // centre of plane k+1 is window slot 1 after the shift
 #pragma unroll
           for (int v = 0; v < 5; ++v) sP[v * PLANE + (H + ty) * PW + (H + tx)] = zw[1][v];
         }
       }
-      if (more_xy) {
+      if (more_xy && !C::BOXA) {
 #pragma unroll
         for (int sidx = 0; sidx < C::NPS; ++sidx) {
           if (lsp[sidx] >= 0) {
