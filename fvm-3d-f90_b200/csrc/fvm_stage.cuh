@@ -944,9 +944,51 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           sd.rc = sN[6 * NN + n];
           return sd;
         };
-        for (int w = tid; w < NF; w += NT) {
-          R F[5];
-          if constexpr (C::SP) {
+        // face states: x face f (cell f on its right) of tile row `row`, and
+        // y face f (cell row f above it) of tile column `col`
+        auto xstates = [&](int f, int row, Prim5<R>& L, Prim5<R>& Rr) {
+          if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
+            const int nl = row * (TX + 2) + f, nr = nl + 1;
+            L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
+            L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
+            const int o = (TB || RECON == RECON_MUSCL_) ? 5 : 0;
+            Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
+            Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
+          } else {
+            const int base = (H + row) * PW + (H + f);  // cell f (right of the face)
+            R l[5], r[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              l[v] = sP[v * PLANE + base - 1];
+              r[v] = sP[v * PLANE + base];
+            }
+            L = mkprim(l);
+            Rr = mkprim(r);
+          }
+        };
+        auto ystates = [&](int f, int col, Prim5<R>& L, Prim5<R>& Rr) {
+          if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
+            const int nl = C::NXN + f * TX + col, nr = nl + TX;
+            L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
+            L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
+            const int o = (TB || RECON == RECON_MUSCL_) ? 5 : 0;
+            Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
+            Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
+          } else {
+            const int base = (H + f) * PW + (H + col);
+            R l[5], r[5];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              l[v] = sP[v * PLANE + base - PW];
+              r[v] = sP[v * PLANE + base];
+            }
+            L = mkprim(l);
+            Rr = mkprim(r);
+          }
+        };
+        if constexpr (C::SP) {
+          for (int w = tid; w < NF; w += NT) {
+            R F[5];
             if (w < C::NXF) {
               const int f = w % (TX + 1), row = w / (TX + 1);
               const int nl = row * (TX + 2) + f;
@@ -957,54 +999,46 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
               const int nl = C::NXN + f * TX + col;
               flux_ausm_sides<1, R>(load_side(nl), load_side(nl + TX), F);
             }
-          } else if (w < C::NXF) {
-            const int f = w % (TX + 1), row = w / (TX + 1);
-            Prim5<R> L, Rr;
-            if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
-              const int nl = row * (TX + 2) + f, nr = nl + 1;
-              L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
-              L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
-              const int o = (TB || RECON == RECON_MUSCL_) ? 5 : 0;
-              Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
-              Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
-            } else {
-              const int base = (H + row) * PW + (H + f);  // cell f (right of the face)
-              R l[5], r[5];
 #pragma unroll
-              for (int v = 0; v < 5; ++v) {
-                l[v] = sP[v * PLANE + base - 1];
-                r[v] = sP[v * PLANE + base];
-              }
-              L = mkprim(l);
-              Rr = mkprim(r);
-            }
-            face_flux<FLUX, 0, R, EX>(L, Rr, K, F);
-          } else {
-            const int w2 = w - C::NXF;
-            const int col = w2 % TX, f = w2 / TX;
-            Prim5<R> L, Rr;
-            if constexpr (RECON == RECON_WENO_ || RECON == RECON_MUSCL_) {
-              const int nl = C::NXN + f * TX + col, nr = nl + TX;
-              L.r = sN[0 * NN + nl]; L.u = sN[1 * NN + nl]; L.v = sN[2 * NN + nl];
-              L.w = sN[3 * NN + nl]; L.p = sN[4 * NN + nl];
-              const int o = (TB || RECON == RECON_MUSCL_) ? 5 : 0;
-              Rr.r = sN[(o + 0) * NN + nr]; Rr.u = sN[(o + 1) * NN + nr]; Rr.v = sN[(o + 2) * NN + nr];
-              Rr.w = sN[(o + 3) * NN + nr]; Rr.p = sN[(o + 4) * NN + nr];
-            } else {
-              const int base = (H + f) * PW + (H + col);
-              R l[5], r[5];
-#pragma unroll
-              for (int v = 0; v < 5; ++v) {
-                l[v] = sP[v * PLANE + base - PW];
-                r[v] = sP[v * PLANE + base];
-              }
-              L = mkprim(l);
-              Rr = mkprim(r);
-            }
-            face_flux<FLUX, 1, R, EX>(L, Rr, K, F);
+            for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
           }
+        } else {
+          // each column thread computes the low x face and the low y face of
+          // its cell in one straight-line block, so the two flux chains
+          // interleave; the tile's high-edge faces (TY x faces, TX y faces)
+          // follow on TY + TX threads
+          if (tid < NC) {
+            const int cx = tid % TX, cy = tid / TX;
+            Prim5<R> Lx, Rx, Ly, Ry;
+            R Fx[5], Fy[5];
+            xstates(cx, cy, Lx, Rx);
+            ystates(cy, cx, Ly, Ry);
+            face_flux<FLUX, 0, R, EX>(Lx, Rx, K, Fx);
+            face_flux<FLUX, 1, R, EX>(Ly, Ry, K, Fy);
+            const int wx = cy * (TX + 1) + cx, wy = C::NXF + cy * TX + cx;
 #pragma unroll
-          for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
+            for (int v = 0; v < 5; ++v) {
+              sF[v * NF + wx] = Fx[v];
+              sF[v * NF + wy] = Fy[v];
+            }
+          }
+          static_assert(TY + TX <= NT && NC <= NT, "edge faces need TY + TX threads");
+          if (tid < TY + TX) {
+            R F[5];
+            Prim5<R> L, Rr;
+            int w;
+            if (tid < TY) {
+              xstates(TX, tid, L, Rr);
+              face_flux<FLUX, 0, R, EX>(L, Rr, K, F);
+              w = tid * (TX + 1) + TX;
+            } else {
+              ystates(TY, tid - TY, L, Rr);
+              face_flux<FLUX, 1, R, EX>(L, Rr, K, F);
+              w = C::NXF + TY * TX + (tid - TY);
+            }
+#pragma unroll
+            for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
+          }
         }
       }
       __syncthreads();
