@@ -987,17 +987,31 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
           }
         };
         if constexpr (C::SP) {
-          for (int w = tid; w < NF; w += NT) {
+          // as below: the cell's low x and y faces together, then the edges
+          if (tid < NC) {
+            const int cx = tid % TX, cy = tid / TX;
+            R Fx[5], Fy[5];
+            const int nlx = cy * (TX + 2) + cx, nly = C::NXN + cy * TX + cx;
+            flux_ausm_sides<0, R>(load_side(nlx), load_side(nlx + 1), Fx);
+            flux_ausm_sides<1, R>(load_side(nly), load_side(nly + TX), Fy);
+            const int wx = cy * (TX + 1) + cx, wy = C::NXF + cy * TX + cx;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              sF[v * NF + wx] = Fx[v];
+              sF[v * NF + wy] = Fy[v];
+            }
+          }
+          if (tid < TY + TX) {
             R F[5];
-            if (w < C::NXF) {
-              const int f = w % (TX + 1), row = w / (TX + 1);
-              const int nl = row * (TX + 2) + f;
+            int w;
+            if (tid < TY) {
+              const int nl = tid * (TX + 2) + TX;
               flux_ausm_sides<0, R>(load_side(nl), load_side(nl + 1), F);
+              w = tid * (TX + 1) + TX;
             } else {
-              const int w2 = w - C::NXF;
-              const int col = w2 % TX, f = w2 / TX;
-              const int nl = C::NXN + f * TX + col;
+              const int nl = C::NXN + TY * TX + (tid - TY);
               flux_ausm_sides<1, R>(load_side(nl), load_side(nl + TX), F);
+              w = C::NXF + TY * TX + (tid - TY);
             }
 #pragma unroll
             for (int v = 0; v < 5; ++v) sF[v * NF + w] = F[v];
