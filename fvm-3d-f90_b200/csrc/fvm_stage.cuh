@@ -882,30 +882,53 @@ __device__ __forceinline__ void stage_run(const StageArgs& a) {
         }
         if (do_xy) {
           constexpr int NN = C::NXN + C::NYN;
-          for (int w = tid; w < NN; w += NT) {
-            R p[5][3], qr[5], ql[5];
-            if (w < C::NXN) {
-              const int c = w % (TX + 2) - 1, row = w / (TX + 2);
-              const int base = (H + row) * PW + (H + c);
+          // x node c (-1..TX) of tile row `row`, y node c (-1..TY) of tile
+          // column `col`: stencil and node-array index
+          auto xnode = [&](int c, int row, R (&p)[5][3]) {
+            const int base = (H + row) * PW + (H + c);
 #pragma unroll
-              for (int v = 0; v < 5; ++v)
+            for (int v = 0; v < 5; ++v)
 #pragma unroll
-                for (int s = 0; s < 3; ++s) p[v][s] = sP[v * PLANE + base + s - 1];
-            } else {
-              const int w2 = w - C::NXN;
-              const int col = w2 % TX, c = w2 / TX - 1;
-              const int base = (H + c) * PW + (H + col);
+              for (int s = 0; s < 3; ++s) p[v][s] = sP[v * PLANE + base + s - 1];
+            return row * (TX + 2) + c + 1;
+          };
+          auto ynode = [&](int c, int col, R (&p)[5][3]) {
+            const int base = (H + c) * PW + (H + col);
 #pragma unroll
-              for (int v = 0; v < 5; ++v)
+            for (int v = 0; v < 5; ++v)
 #pragma unroll
-                for (int s = 0; s < 3; ++s) p[v][s] = sP[v * PLANE + base + (s - 1) * PW];
-            }
-            node(p, qr, ql);
+              for (int s = 0; s < 3; ++s) p[v][s] = sP[v * PLANE + base + (s - 1) * PW];
+            return C::NXN + (c + 1) * TX + col;
+          };
+          auto put = [&](int w, const R (&qr)[5], const R (&ql)[5]) {
 #pragma unroll
             for (int v = 0; v < 5; ++v) {
               sN[v * NN + w] = qr[v];
               sN[(5 + v) * NN + w] = ql[v];
             }
+          };
+          // each column thread: the x node and the y node of its own cell in
+          // one straight-line block (independent chains); then the tile's
+          // edge nodes (x nodes -1 and TX of each row, y nodes -1 and TY of
+          // each column) on 2 (TX + TY) threads
+          static_assert(2 * (TX + TY) <= NT && NC <= NT, "edge nodes need 2 (TX + TY) threads");
+          if (tid < NC) {
+            R px[5][3], py[5][3], qrx[5], qlx[5], qry[5], qly[5];
+            const int wx = xnode(tx, ty, px), wy = ynode(ty, tx, py);
+            node(px, qrx, qlx);
+            node(py, qry, qly);
+            put(wx, qrx, qlx);
+            put(wy, qry, qly);
+          }
+          if (tid < 2 * (TX + TY)) {
+            R p[5][3], qr[5], ql[5];
+            int w;
+            if (tid < 2 * TY)
+              w = xnode(tid < TY ? -1 : TX, tid % TY, p);
+            else
+              w = ynode(tid < 2 * TY + TX ? -1 : TY, (tid - 2 * TY) % TX, p);
+            node(p, qr, ql);
+            put(w, qr, ql);
           }
           __syncthreads();
         }
